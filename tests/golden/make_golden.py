@@ -1,0 +1,340 @@
+"""Generate the golden fixtures by running the REFERENCE implementation.
+
+Run in the development container, where the reference package
+(``specific_particle_tracer`` from AdamCBartnik/BEM) is importable from its
+source tree:
+
+    python tests/golden/make_golden.py [--ref /path/to/reference] [names...]
+
+It puts ``tests/golden/_stub`` (a minimal ParticleGroup stand-in, since
+openpmd-beamphysics is not installed) and the reference tree on sys.path,
+calls the reference's own functions on seeded inputs, and writes one
+compressed ``.npz`` per fixture next to this script.  The GPU box never
+runs this; tests only read the ``.npz`` files.
+"""
+
+import argparse
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def _setup(ref):
+    sys.path.insert(0, os.path.join(HERE, "_stub"))
+    sys.path.insert(0, ref)
+    sys.path.insert(0, REPO)
+
+
+def _save(name, **arrays):
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **arrays)
+    print(f"wrote {path} ({os.path.getsize(path)} bytes)")
+
+
+def gen_ellip():
+    from specific_particle_tracer.bem._elliptic import ellip_ke_complement
+    p = np.concatenate([np.logspace(-300, -1, 400), np.linspace(0.1, 1.0, 200), [1.0, 0.5, 1e-3, 1e-3 * (1 + 1e-15)]])
+    K, E = ellip_ke_complement(p, np)
+    _save("ellip", p=p, K=K, E=E)
+
+
+def gen_ring():
+    from specific_particle_tracer.bem.axisymmetric import ring_field
+    rng = np.random.default_rng(11)
+    n = 600
+    a = rng.uniform(1e-9, 1e-7, n)
+    rho = a * np.exp(rng.uniform(-3, 3, n))
+    z = a * rng.normal(0, 1.0, n)
+    # near the ring itself, near the axis, exactly on the axis
+    rho[:100] = a[:100] * (1 + rng.normal(0, 1e-3, 100))
+    z[:100] = a[:100] * rng.normal(0, 1e-3, 100)
+    rho[100:150] = a[100:150] * 1e-6
+    rho[150:170] = 0.0
+    er, ez = ring_field(rho, z, a, np)
+    _save("ring", rho=rho, z=z, a=a, er=er, ez=ez)
+
+
+def _states(rng, G, E, scale, zoff=0.0, live_frac=0.8):
+    pos = rng.normal(0, scale, (G, E, 3))
+    pos[..., 2] = np.abs(pos[..., 2]) + zoff
+    vel = rng.normal(0, 1e5, (G, E, 3))
+    live = rng.uniform(0, 1, (G, E)) < live_frac
+    return pos, vel, live
+
+
+def gen_accel():
+    from specific_particle_tracer import geometry as g
+    from specific_particle_tracer.constants import ELEMENTARY_CHARGE, ev_to_kg
+    rng = np.random.default_rng(12)
+    m = ev_to_kg(510998.95069)
+    out = {}
+    for name, geo, scale, zoff in [
+        ("flat", g.FlatCathode(-1e7, z0=3e-9), 5e-8, 0.0),
+        ("flat_noimg", g.FlatCathode(-1e7, z0=None), 5e-8, 0.0),
+        ("tip", g.HemisphericalTip(-1e8, 50e-9, z0=3e-9), 3e-8, 50e-9),
+    ]:
+        G, E = 3, 7
+        pos, vel, live = _states(rng, G, E, scale, zoff)
+        charge = np.full((G, E), -ELEMENTARY_CHARGE)
+        mass = np.full((G, E), m)
+        acc = g.make_accel_fn(charge, mass, -ELEMENTARY_CHARGE / m, geo, 1e-12)(pos, vel, live, np.arange(G))
+        kill = g.make_kill_fn(geo, 1e-6)(pos)
+        out.update({f"{name}_pos": pos, f"{name}_vel": vel, f"{name}_live": live, f"{name}_acc": acc,
+                    f"{name}_kill": kill})
+    _save("accel", **out)
+
+
+def _surface_points(rng, profile, n, out_scale):
+    """Points on, just off, and away from the profile's surface of revolution."""
+    prof = np.asarray(profile)
+    seg = rng.integers(0, len(prof) - 1, n)
+    t = rng.uniform(0, 1, n)
+    p = prof[seg] + t[:, None] * (prof[seg + 1] - prof[seg])
+    tan = prof[seg + 1] - prof[seg]
+    nrm = np.stack([-tan[:, 1], tan[:, 0]], -1)
+    nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
+    k = np.arange(n) % 4
+    off = np.where(k == 0, 0.0, np.where(k == 1, 1e-3, np.where(k == 2, 0.3, 3.0))) * out_scale
+    rz = p + off[:, None] * nrm
+    ph = rng.uniform(0, 2 * np.pi, n)
+    pts = np.stack([rz[:, 0] * np.cos(ph), rz[:, 0] * np.sin(ph), rz[:, 1]], -1)
+    return pts
+
+
+def gen_bem_sphere():
+    from specific_particle_tracer.bem.geometry import HemisphericalTipBEMGeometry
+    rng = np.random.default_rng(13)
+    R = 50e-9
+    geo = HemisphericalTipBEMGeometry(-1e8, R, field_max_length=R * np.pi / 40)
+    sol = geo.field_solver.solution
+    pts = _surface_points(rng, sol.profile, 64, R / 40)
+    pts = np.concatenate([pts, [[0, 0, R], [0, 0, 1.5 * R], [1e-12, 0, 2 * R], [3 * R, 0, 5 * R],
+                                [0, 0, 15 * R], [2 * R, 1 * R, 12 * R], [0, 0, 25 * R]]])
+    pts = pts[pts[:, 2] >= 0]
+    e_pert = sol.field(pts)
+    e_geo = geo.field(pts[None])[0]
+    kill = geo.kill_mask(pts)
+    _save("bem_sphere", profile=sol.profile, sigma=sol.sigma, R=R, E_gun=-1e8, z_handoff=geo.z_handoff,
+          n_subdiv=geo.n_subdiv, points=pts, e_pert=e_pert, e_geo=e_geo, kill=kill)
+
+
+def gen_bem_well():
+    from specific_particle_tracer.bem.geometry import CylindricalWellBEMGeometry
+    rng = np.random.default_rng(14)
+    R, H = 2e-6, 1e-6
+    geo = CylindricalWellBEMGeometry(-2.5e6, R, H, field_max_length=H / 6)
+    sol = geo.field_solver.solution
+    pts = _surface_points(rng, sol.profile[: len(sol.profile) // 2], 48, H / 6)
+    pts = np.concatenate([pts, [[0, 0, -H], [0, 0, -0.5 * H], [0.5 * R, 0, 0.0], [3 * R, 0, 5 * H], [0, 0, 30 * H]]])
+    e_pert = sol.field(pts)
+    e_geo = geo.field(pts[None])[0]
+    kill = geo.kill_mask(pts)
+    _save("bem_well", profile=sol.profile, sigma=sol.sigma, R=R, H=H, E_gun=-2.5e6, z_handoff=geo.z_handoff,
+          n_subdiv=geo.n_subdiv, points=pts, e_pert=e_pert, e_geo=e_geo, kill=kill)
+
+
+class _PostTip:
+    """Hemisphere on a post, composed only of reference functions: BEM field
+    of the mirror-doubled capsule (AxisymmetricBEMSolution), blend with the
+    flat fallback (bem.geometry._blend_with_flat_fallback), 3-image force of
+    forces.hemispherical_tip_image_force in the apex frame."""
+
+    def __init__(self, E_gun, R, L, profile, z0, z_handoff, n_subdiv=8):
+        from specific_particle_tracer.bem.axisymmetric import AxisymmetricBEMSolution
+        from specific_particle_tracer.fields import GunField
+        self.E_gun, self.R, self.L, self.z0, self.z_handoff, self.n_subdiv = E_gun, R, L, z0, z_handoff, n_subdiv
+        self.solution = AxisymmetricBEMSolution.solve(profile, dirichlet_fn=lambda rho, z: E_gun * z)
+        self.gun = GunField(E_gun)
+
+    def inside(self, pos):
+        rk = self.R * (1.0 - 1e-6)
+        x, y, z = pos[..., 0], pos[..., 1], pos[..., 2]
+        return ((x * x + y * y <= rk * rk) & (z <= self.L)) | (x * x + y * y + (z - self.L) ** 2 <= rk * rk)
+
+    def field(self, pos):
+        from specific_particle_tracer.bem.geometry import _blend_with_flat_fallback
+        ok = (~self.inside(pos)) & (pos[..., 2] >= 0.0)
+        uni = np.zeros_like(pos)
+        uni[..., 2] = self.E_gun
+        near = np.where(ok[..., None], uni + self.solution.field(pos, n_subdiv=self.n_subdiv), 0.0)
+        return _blend_with_flat_fallback(near, self.gun.evaluate(pos), pos[..., 2], 0.5 * self.z_handoff,
+                                         self.z_handoff, np)
+
+    def image_force(self, pos, charge, active, soft):
+        from specific_particle_tracer.forces import hemispherical_tip_image_force
+        sh = pos.copy()
+        sh[..., 2] -= self.L
+        return hemispherical_tip_image_force(sh, charge, active, self.R - self.z0, soft,
+                                             plane_z0=self.L + self.z0, xp=np)
+
+    def kill_mask(self, pos):
+        return self.inside(pos) | (pos[..., 2] <= 0.0)
+
+
+def _post_case():
+    from bem_b200.mesh import capsule_profile
+    R, L = 50e-9, 400e-9
+    prof = capsule_profile(R, L, 10, 20)
+    return _PostTip(-1e7, R, L, prof, 3e-9, 20 * (L + R))
+
+
+def gen_bem_post():
+    rng = np.random.default_rng(15)
+    geo = _post_case()
+    sol = geo.solution
+    pts = _surface_points(rng, sol.profile[: len(sol.profile) // 2], 48, 5e-9)
+    pts = pts[pts[:, 2] >= 0]
+    e_pert = sol.field(pts)
+    e_geo = geo.field(pts[None])[0]
+    _save("bem_post", profile=sol.profile, sigma=sol.sigma, R=geo.R, L=geo.L, E_gun=geo.E_gun, z0=geo.z0,
+          z_handoff=geo.z_handoff, n_subdiv=8, points=pts, e_pert=e_pert, e_geo=e_geo, kill=geo.kill_mask(pts))
+
+
+def _trace(geo, pos0, vel0, tb, t_max, rtol, atol, z_max, soft=1e-12):
+    from specific_particle_tracer import batched_rk45, geometry as g
+    from specific_particle_tracer.constants import ELEMENTARY_CHARGE, ev_to_kg
+    G, E, _ = pos0.shape
+    m = ev_to_kg(510998.95069)
+    charge = np.full((G, E), -ELEMENTARY_CHARGE)
+    mass = np.full((G, E), m)
+    acc = g.make_accel_fn(charge, mass, -ELEMENTARY_CHARGE / m, geo, soft)
+    calls = np.zeros(G, dtype=np.int64)
+
+    def counted(pos, vel, active, gidx):
+        calls[gidx] += 1
+        return acc(pos, vel, active, gidx)
+
+    steps = [[] for _ in range(G)]
+
+    def on_step(gi, t_old, p_old, v_old, t_new, p_new, v_new):
+        for k, gg in enumerate(gi):
+            steps[gg].append(t_new[k])
+
+    kill = g.make_kill_fn(geo, z_max)
+    t0 = time.time()
+    pos, vel = batched_rk45.integrate(counted, pos0, vel0, tb, t_max, rtol, atol, on_step=on_step, kill_fn=kill)
+    print(f"  trace {G}x{E}: {time.time() - t0:.1f}s, attempts {calls // 7}")
+    n_acc = np.array([len(s) for s in steps])
+    t_acc = np.zeros((G, n_acc.max()))
+    for k, s in enumerate(steps):
+        t_acc[k, :len(s)] = s
+    return dict(pos0=pos0, vel0=vel0, t_birth=tb, t_max=t_max, rtol=rtol, atol=atol, z_max=z_max,
+                pos=pos, vel=vel, attempts=calls // 7, n_acc=n_acc, t_acc=t_acc)
+
+
+def _grouped(d, G, E, mass):
+    from specific_particle_tracer.constants import ev_c_to_si_momentum
+    sl = slice(0, G * E)
+    pos = np.stack([d["x"][sl], d["y"][sl], d["z"][sl]], -1).reshape(G, E, 3)
+    vel = np.stack([ev_c_to_si_momentum(d[k][sl]) / mass for k in ("px", "py", "pz")], -1).reshape(G, E, 3)
+    return pos, vel, d["t"][sl].reshape(G, E)
+
+
+def gen_trace_flat(n_groups=2):
+    from specific_particle_tracer import geometry as g
+    from specific_particle_tracer.constants import ev_to_kg
+    from bem_b200 import workloads as w
+    d = w.flat_c0()
+    pos, vel, tb = _grouped(d, n_groups, 64, ev_to_kg(510998.95069))
+    t_max = w.default_t_max(-1e7, 1e-3, 1e-12)
+    res = _trace(g.FlatCathode(-1e7, z0=3e-9, kill_z_below=0.0), pos, vel, tb, t_max, 1e-8, 1e-12, 1e-3)
+    _save("trace_flat" if n_groups == 2 else "trace_flat_c0", **res)
+
+
+def gen_trace_tip():
+    from specific_particle_tracer import geometry as g
+    from specific_particle_tracer.constants import ev_to_kg
+    from bem_b200 import workloads as w
+    R = 50e-9
+    d = w.tip_c2(n_groups=2, n_emit=12, R=R, L=0.0, seed=21)
+    pos, vel, tb = _grouped(d, 2, 12, ev_to_kg(510998.95069))
+    res = _trace(g.HemisphericalTip(-1e8, R, z0=3e-9), pos, vel, tb, 2e-12, 1e-8, 1e-12, 2e-6)
+    _save("trace_tip", **res)
+
+
+def gen_trace_bem():
+    from specific_particle_tracer.bem.geometry import HemisphericalTipBEMGeometry
+    from specific_particle_tracer.constants import ev_to_kg
+    from bem_b200 import workloads as w
+    R = 50e-9
+    geo = HemisphericalTipBEMGeometry(-1e8, R, field_max_length=R * np.pi / 30)
+    d = w.tip_c2(n_groups=1, n_emit=4, R=R, L=0.0, seed=22, t_spread=0.2e-12)
+    pos, vel, tb = _grouped(d, 1, 4, ev_to_kg(510998.95069))
+    res = _trace(geo, pos, vel, tb, 0.4e-12, 1e-8, 1e-12, 3e-7)
+    sol = geo.field_solver.solution
+    _save("trace_tip_bem", profile=sol.profile, sigma=sol.sigma, R=R, E_gun=-1e8, z_handoff=geo.z_handoff,
+          n_subdiv=8, **res)
+
+
+def gen_trace_post():
+    from specific_particle_tracer.constants import ev_to_kg
+    from bem_b200 import workloads as w
+    geo = _post_case()
+    d = w.tip_c2(n_groups=1, n_emit=4, R=geo.R, L=geo.L, seed=23, t_spread=0.2e-12)
+    pos, vel, tb = _grouped(d, 1, 4, ev_to_kg(510998.95069))
+    res = _trace(geo, pos, vel, tb, 0.4e-12, 1e-8, 1e-12, 2e-6)
+    _save("trace_post", profile=geo.solution.profile, sigma=geo.solution.sigma, R=geo.R, L=geo.L,
+          E_gun=geo.E_gun, z0=geo.z0, z_handoff=geo.z_handoff, n_subdiv=8, **res)
+
+
+def gen_trace_well():
+    from specific_particle_tracer.bem.geometry import CylindricalWellBEMGeometry
+    from specific_particle_tracer.constants import ev_to_kg
+    from bem_b200 import workloads as w
+    R, H = 2e-6, 1e-6
+    geo = CylindricalWellBEMGeometry(-2.5e7, R, H, field_max_length=H / 6)
+    d = w.well_c3(n_groups=40, seed=24, R=R, H=H, t_spread=0.5e-12)
+    n = 3
+    pos, vel, tb = _grouped(d, 1, n, ev_to_kg(510998.95069))
+    res = _trace(geo, pos, vel, tb, 1.0e-12, 1e-8, 1e-12, 5e-6)
+    sol = geo.field_solver.solution
+    _save("trace_well", profile=sol.profile, sigma=sol.sigma, R=R, H=H, E_gun=-2.5e7, z_handoff=geo.z_handoff,
+          n_subdiv=8, **res)
+
+
+def gen_tracker():
+    """Tracker-level outputs (screens, t_out) for a small flat case."""
+    from specific_particle_tracer import SpecificParticleTracer, geometry as g
+    from beamphysics import ParticleGroup
+    from bem_b200 import workloads as w
+    d = w.flat_c0(n_groups=3, n_emit=6, seed=31)
+    pg = ParticleGroup(data={k: v for k, v in d.items() if k != "group_sizes"})
+    tr = SpecificParticleTracer(pg, 6, g.FlatCathode(-1e7), screens=[1e-7, 5e-6], t_out=[0.5e-12, 1.5e-12],
+                                rtol=1e-8, z_max=2e-5)
+    scr, trj = tr.run()
+    out = dict(t_max=tr.t_max)
+    for k, s in enumerate(scr):
+        for key in ("x", "y", "z", "px", "py", "pz", "t", "id"):
+            out[f"screen{k}_{key}"] = np.asarray(getattr(s, key))
+    for k, s in enumerate(trj):
+        for key in ("x", "y", "z", "px", "py", "pz", "t", "id"):
+            out[f"traj{k}_{key}"] = np.asarray(getattr(s, key))
+    _save("tracker_flat", **out)
+
+
+GENERATORS = dict(ellip=gen_ellip, ring=gen_ring, accel=gen_accel, bem_sphere=gen_bem_sphere,
+                  bem_well=gen_bem_well, bem_post=gen_bem_post, trace_flat=gen_trace_flat,
+                  trace_tip=gen_trace_tip, trace_tip_bem=gen_trace_bem, trace_post=gen_trace_post,
+                  trace_well=gen_trace_well, tracker=gen_tracker,
+                  trace_flat_c0=lambda: gen_trace_flat(16))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("names", nargs="*")
+    a = ap.parse_args()
+    _setup(a.ref)
+    for name in a.names or [k for k in GENERATORS if k != "trace_flat_c0"]:
+        t0 = time.time()
+        GENERATORS[name]()
+        print(f"{name}: {time.time() - t0:.1f}s")
+
+
+if __name__ == "__main__":
+    main()
