@@ -1,0 +1,1310 @@
+// B200 (sm_100a) kernels for the specific_particle_tracer hot path.
+//
+// One persistent kernel (trace_kernel) advances emission groups through the
+// per-group adaptive Dormand-Prince 5(4) integrator of batched_rk45.py.  A
+// CTA owns one group at a time (groups come from a device work queue); the
+// group's state, its seven stage slopes and the stage positions live in
+// shared memory, so a step attempt never leaves the SM.  Every stage
+// evaluates, on the stage positions:
+//   * the external field: analytic (fields.py) or the BEM ring-charge sum
+//     blended with the flat fallback (bem/axisymmetric.py, bem/geometry.py),
+//   * Plummer-softened Coulomb pair forces within the group (forces.py:16-57),
+//   * the image-charge pair forces (forces.py:60-191).
+//
+// BEM field of a list of points (bem_points):
+//   A. closest segment per point: one warp per point, lanes stride the
+//      segment table, warp-shuffle argmin (ties -> lowest index, the
+//      strict-< rule of bem/axisymmetric.py:127), on-surface offset;
+//   B. near segments (distance < segment length): found by a lane-parallel
+//      test + ballot; each near segment is integrated by the whole warp with
+//      the sinh-mapped Gauss-8 rule (lanes over interval x node);
+//   C. far sum: the Gauss-4 node table streams through shared memory in
+//      tiles copied by the TMA bulk engine (cp.async.bulk + mbarrier, double
+//      buffered); up to 8 points per round, every thread owns a strided
+//      slice of each tile and keeps 8 (E_rho, E_z) accumulators; near
+//      segments are skipped by a per-(point, segment) flag; one fixed-order
+//      block reduction per round (bit-reproducible run to run).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include <math.h>
+#include <stdarg.h>
+
+#include "../../include/spt_b200.h"
+#include "spt_math.cuh"
+
+namespace spt {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kRound = 8;           // points per far-sum round
+constexpr int kTileNodes = 1024;    // nodes per TMA tile
+constexpr int kSmallGroup = 256;    // groups above this keep slopes in global memory
+
+// Dormand-Prince 5(4) tableau (batched_rk45.py:30-50).
+__device__ __constant__ double kA[6][5] = {
+    {0, 0, 0, 0, 0},
+    {1.0 / 5, 0, 0, 0, 0},
+    {3.0 / 40, 9.0 / 40, 0, 0, 0},
+    {44.0 / 45, -56.0 / 15, 32.0 / 9, 0, 0},
+    {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729, 0},
+    {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656}};
+__device__ __constant__ double kB[6] = {35.0 / 384, 0.0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84};
+__device__ __constant__ double kE[7] = {71.0 / 57600, 0.0, -71.0 / 16695, 71.0 / 1920, -17253.0 / 339200, 22.0 / 525, -1.0 / 40};
+
+constexpr double kSpeedOfLight = 299792458.0;
+constexpr double kTiny = 2.2250738585072014e-308;  // np.finfo(float).tiny
+
+// ---------------------------------------------------------------------------
+// small helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// Bounded wait on an mbarrier phase.  Returns false when the iteration limit
+// ran out (the caller flags the group instead of spinning forever).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
+    uint32_t done = 0;
+    for (int it = 0; it < (1 << 24); ++it) {
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(phase)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// geometry helpers (fields.py, geometry.py, bem/fields.py, bem/geometry.py)
+
+__device__ __forceinline__ bool well_contains(double rho, double z, const SptGeometry& g) {
+    const double R = g.R, H = g.H;
+    const double eps = 1e-6 * R;
+    bool solid = (rho >= R * (1.0 - 1e-6)) ? (z <= 0.0) : (z <= -H * (1.0 + 1e-6));
+    if (g.rim_fillet > 0.0) {
+        const double rf = g.rim_fillet, cr = R + rf, cz = -rf;
+        if (rho >= R - eps && rho <= R + rf + eps && z >= -rf - eps && z <= eps) solid = hypot(rho - cr, z - cz) <= rf;
+    }
+    if (g.bottom_fillet > 0.0) {
+        const double bf = g.bottom_fillet, cr = R - bf, cz = -H + bf;
+        if (rho <= R + eps && rho >= R - bf - eps && z <= -H + bf + eps && z >= -H - eps)
+            solid = hypot(rho - cr, z - cz) >= bf;
+    }
+    return solid;
+}
+
+__device__ __forceinline__ bool post_inside(double x, double y, double z, const SptGeometry& g) {
+    const double rk = g.R * (1.0 - 1e-6);
+    const double r2 = x * x + y * y;
+    const double zc = z - g.L;
+    return (r2 <= rk * rk && z <= g.L) || (r2 + zc * zc <= rk * rk);
+}
+
+template <int KIND>
+__device__ __forceinline__ bool kill_test(double x, double y, double z, const SptGeometry& g) {
+    bool k = false;
+    if (KIND == SPT_GEOM_FLAT) {
+        k = g.has_kill_below && z <= g.kill_z_below;
+    } else if (KIND == SPT_GEOM_TIP || KIND == SPT_GEOM_TIP_BEM) {
+        const double rk = g.R * (1.0 - 1e-6);
+        k = (x * x + y * y + z * z) <= rk * rk;
+        if (g.has_kill_below) k = k || (z <= g.kill_z_below);
+    } else if (KIND == SPT_GEOM_WELL_BEM) {
+        k = well_contains(sqrt(x * x + y * y), z, g);
+    } else {
+        k = post_inside(x, y, z, g);
+        if (g.has_kill_below) k = k || (z <= g.kill_z_below);
+    }
+    if (g.has_z_max) k = k || (z >= g.z_max);
+    return k;
+}
+
+// analytic tip field (fields.py:119-160)
+__device__ __forceinline__ void tip_field(double x, double y, double z, double Ez, double R, double& ex, double& ey,
+                                          double& ez) {
+    const double r = sqrt(x * x + y * y + z * z);
+    const bool ok = (r >= R * (1.0 - 1e-6)) && (z >= 0.0);
+    if (!ok) {
+        ex = ey = ez = 0.0;
+        return;
+    }
+    const double r3 = r * r * r;
+    const double r5 = r3 * r * r;
+    const double R3 = R * R * R;
+    ex = 3.0 * Ez * R3 * x * z / r5;
+    ey = 3.0 * Ez * R3 * y * z / r5;
+    ez = Ez * (1.0 - R3 / r3 + 3.0 * R3 * z * z / r5);
+}
+
+// BEM geometries: is the point in the field's valid (vacuum) region
+template <int KIND>
+__device__ __forceinline__ bool bem_valid(double x, double y, double z, const SptGeometry& g) {
+    if (KIND == SPT_GEOM_TIP_BEM) return (sqrt(x * x + y * y + z * z) >= g.R * (1.0 - 1e-6)) && (z >= 0.0);
+    if (KIND == SPT_GEOM_WELL_BEM) return !well_contains(sqrt(x * x + y * y), z, g);
+    return !post_inside(x, y, z, g) && (z >= 0.0);
+}
+
+__device__ __forceinline__ double blend_weight(double z, double zh) {
+    const double zlo = 0.5 * zh;
+    double s = (zh - z) / (zh - zlo);
+    s = fmin(fmax(s, 0.0), 1.0);
+    return s * s * (3.0 - 2.0 * s);
+}
+
+// ---------------------------------------------------------------------------
+// shared-memory layout of one CTA
+
+struct Layout {
+    // offsets in doubles from the start of dynamic shared memory
+    int y0, nw, sp, kp, kv;   // y0: 6E, nw: 6E, sp: 3E, kp/kv: 21E each
+    int tb, td, q, m, cps;    // E each
+    int fld;                  // 3E field
+    int img;                  // 4E sphere images
+    int bpt;                  // 8E per BEM list entry: x y z rho_e z_e near_r near_z (+1 pad)
+    int tiles;                // 2 * 3 * kTileNodes
+    int red;                  // kWarps * 2 * kRound
+    int ints;                 // int region start (in doubles)
+    int total_doubles;
+    int live_off, list_off, flags_off;  // in ints from ints start
+    size_t bytes;
+    bool big;                 // slopes/y0/nw in global memory
+};
+
+__host__ __device__ inline Layout make_layout(int E, bool want_tiles) {
+    Layout L;
+    const bool big = E > kSmallGroup;
+    int o = 0;
+    L.big = big;
+    if (!big) {
+        L.y0 = o; o += 6 * E;
+        L.nw = o; o += 6 * E;
+        L.kp = o; o += 21 * E;
+        L.kv = o; o += 21 * E;
+    } else {
+        L.y0 = L.nw = L.kp = L.kv = -1;
+    }
+    L.sp = o; o += 3 * E;
+    L.tb = o; o += E;
+    L.td = o; o += E;
+    L.q = o; o += E;
+    L.m = o; o += E;
+    L.cps = o; o += E;
+    L.fld = o; o += 3 * E;
+    L.img = o; o += 4 * E;
+    L.bpt = o; o += 8 * E;
+    o = (o + 1) & ~1;  // 16-byte alignment for the TMA tiles
+    L.tiles = o; o += want_tiles ? 2 * 3 * kTileNodes : 0;
+    L.red = o; o += kWarps * 2 * kRound;
+    L.ints = o;
+    L.live_off = 0;
+    L.list_off = E;
+    L.flags_off = 2 * E;
+    const int n_ints = 2 * E + kRound * 256 / 4 + 4;  // live, list, near flags (bytes) packed in ints
+    L.total_doubles = o + (n_ints + 1) / 2;
+    L.bytes = (size_t)L.total_doubles * 8 + 64;  // + mbarriers
+    return L;
+}
+
+// global per-CTA slot for big groups: y0 6E, nw 6E, kp 21E, kv 21E
+__host__ __device__ inline size_t big_slot_doubles(int E) { return (size_t)54 * E; }
+
+struct Ctx {
+    SptGeometry g;
+    SptBem bem;
+    double cm;       // charge_to_mass
+    double kc;       // Coulomb constant 1/(4 pi eps0)
+    double soft2;    // plummer^2
+    int form;
+    int E;
+    double* base;    // dynamic smem
+    Layout L;
+    double *y0, *nw, *sp, *kp, *kv, *tb, *td, *q, *m, *cps, *fld, *img, *bpt, *tiles, *red;
+    int* live;
+    int* list;
+    unsigned char* nflag;
+    uint64_t* bars;
+    unsigned long long cnt[8];  // per-thread counter partials (thread 0 flushes)
+};
+
+__device__ inline void bind(Ctx& c, double* smem, int E, double* slot) {
+    c.base = smem;
+    c.E = E;
+    c.L = make_layout(E, true);
+    const Layout& L = c.L;
+    if (!L.big) {
+        c.y0 = smem + L.y0;
+        c.nw = smem + L.nw;
+        c.kp = smem + L.kp;
+        c.kv = smem + L.kv;
+    } else {
+        c.y0 = slot;
+        c.nw = slot + 6 * E;
+        c.kp = slot + 12 * E;
+        c.kv = slot + 33 * E;
+    }
+    c.sp = smem + L.sp;
+    c.tb = smem + L.tb;
+    c.td = smem + L.td;
+    c.q = smem + L.q;
+    c.m = smem + L.m;
+    c.cps = smem + L.cps;
+    c.fld = smem + L.fld;
+    c.img = smem + L.img;
+    c.bpt = smem + L.bpt;
+    c.tiles = smem + L.tiles;
+    c.red = smem + L.red;
+    int* ib = reinterpret_cast<int*>(smem + L.ints);
+    c.live = ib + L.live_off;
+    c.list = ib + L.list_off;
+    c.nflag = reinterpret_cast<unsigned char*>(ib + L.flags_off);
+    c.bars = reinterpret_cast<uint64_t*>(smem + L.total_doubles + 1);
+    for (int k = 0; k < 8; ++k) c.cnt[k] = 0;
+}
+
+// ---------------------------------------------------------------------------
+// BEM: segment table access
+
+struct Seg {
+    double p0r, p0z, tr, tz, len, ur, uz, nr, nz, s0, s1;
+};
+
+__device__ __forceinline__ double segf(const SptBem& b, int f, int s) { return __ldg(b.seg + (size_t)f * b.seg_stride + s); }
+
+// closest-point distance^2 of (rq, zq) to segment s (bem/axisymmetric.py:117-133)
+__device__ __forceinline__ double seg_dist2(const SptBem& b, int s, double rq, double zq) {
+    const double p0x = segf(b, 0, s), p0y = segf(b, 1, s), ax = segf(b, 2, s), ay = segf(b, 3, s);
+    const double ab = ax * ax + ay * ay;
+    double t = ((rq - p0x) * ax + (zq - p0y) * ay) / ab;
+    t = fmin(fmax(t, 0.0), 1.0);
+    const double cr = p0x + t * ax, cz = p0y + t * ay;
+    const double dr = rq - cr, dz = zq - cz;
+    return dr * dr + dz * dz;
+}
+
+// near test of bem/axisymmetric.py:566-570 -> (near, projection, distance)
+__device__ __forceinline__ bool seg_near(const SptBem& b, int s, double re, double ze, double& proj, double& dist) {
+    const double p0r = segf(b, 0, s), p0z = segf(b, 1, s), L = segf(b, 4, s), ur = segf(b, 5, s), uz = segf(b, 6, s);
+    const double dr = re - p0r, dz = ze - p0z;
+    const double along = dr * ur + dz * uz;
+    proj = fmin(fmax(along, 0.0), L);
+    const double ar = dr - proj * ur, az = dz - proj * uz;
+    dist = sqrt(ar * ar + az * az);
+    return dist < L;
+}
+
+// ---------------------------------------------------------------------------
+// BEM field of the n points listed in c.bpt (x, y, z at slots 0..2 of each
+// 8-double record).  Writes the perturbation field into c.fld[3*list[k]..]
+// when `scatter`, else into bpt record slots 5..7 (ex, ey, ez).
+// Must be called by all threads of the CTA.
+
+__device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
+    const SptBem& b = c.bem;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* P = c.bpt;  // record k: [0]x [1]y [2]z [3]rho_e [4]z_e [5]ax [6]ay [7]near_r ; near_z in fld tmp
+    const int nseg = b.n_seg;
+    const int nps = b.nodes_per_seg;
+
+    // A: closest point + on-surface offset (one warp per point)
+    for (int k = warp; k < n; k += kWarps) {
+        const double x = P[8 * k + 0], y = P[8 * k + 1], z = P[8 * k + 2];
+        const double rho = hypot(x, y);
+        double best = INFINITY;
+        int bs = 0x7fffffff;
+        for (int s = lane; s < nseg; s += 32) {
+            const double d2 = seg_dist2(b, s, rho, z);
+            if (d2 < best) { best = d2; bs = s; }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            const int os = __shfl_xor_sync(0xffffffffu, bs, o);
+            if (ob < best || (ob == best && os < bs)) { best = ob; bs = os; }
+        }
+        if (lane == 0) {
+            if (bs >= nseg) bs = 0;  // every distance was NaN: the reference keeps index 0
+            const double Ls = segf(b, 4, bs);
+            const double off = (best < (1e-9 * Ls) * (1e-9 * Ls)) ? 1e-4 * Ls : 0.0;
+            double re = rho + off * segf(b, 7, bs);
+            if (rho == 0.0) re = 0.0;
+            P[8 * k + 3] = re;
+            P[8 * k + 4] = z + off * segf(b, 8, bs);
+        }
+    }
+    __syncthreads();
+
+    // B: near-segment sinh quadrature (one warp per point)
+    unsigned long long n_near = 0, n_ring_near = 0;
+    for (int k = warp; k < n; k += kWarps) {
+        const double re = P[8 * k + 3], ze = P[8 * k + 4];
+        double acc_r = 0.0, acc_z = 0.0;
+        for (int s0 = 0; s0 < nseg; s0 += 32) {
+            const int s = s0 + lane;
+            double proj = 0.0, dist = 0.0;
+            const bool nr = (s < nseg) && seg_near(b, s, re, ze, proj, dist);
+            unsigned mask = __ballot_sync(0xffffffffu, nr);
+            while (mask) {
+                const int j = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const int sg = s0 + j;
+                const double sp = __shfl_sync(0xffffffffu, proj, j);
+                const double Ls = segf(b, 4, sg);
+                const double d = fmax(__shfl_sync(0xffffffffu, dist, j), 1e-15 * Ls);
+                const double lo = asinh(-sp / d), hi = asinh((Ls - sp) / d);
+                const int cnt = max(1, (int)ceil((hi - lo) / 0.5));
+                const double width = (hi - lo) / cnt;
+                const double half = 0.5 * (hi - lo) / cnt;
+                const double p0r = segf(b, 0, sg), p0z = segf(b, 1, sg), ur = segf(b, 5, sg), uz = segf(b, 6, sg);
+                const double sg0 = segf(b, 9, sg), sg1 = segf(b, 10, sg);
+                for (int qn = lane; qn < cnt * 8; qn += 32) {
+                    const int iv = qn >> 3, gi = qn & 7;
+                    const double v = lo + (iv + 0.5 * (b.gauss8_x[gi] + 1.0)) * width;
+                    const double sl = sp + d * sinh(v);
+                    const double sr = p0r + sl * ur, sz = p0z + sl * uz;
+                    const double dens = sg0 + (sl / Ls) * (sg1 - sg0);
+                    const double w = dens * (2.0 * kPi * sr) * d * cosh(v) * half * b.gauss8_w[gi];
+                    double er, ez;
+                    ring_field(re, ze - sz, sr, er, ez);
+                    acc_r += w * er;
+                    acc_z += w * ez;
+                }
+                if (lane == 0) { n_near += 1; n_ring_near += (unsigned long long)cnt * 8; }
+            }
+        }
+        acc_r = warp_sum(acc_r);
+        acc_z = warp_sum(acc_z);
+        if (lane == 0) {
+            P[8 * k + 7] = acc_r;
+            c.fld[3 * k + 2] = acc_z;  // temporary near_z (fld is rewritten after the far sum)
+        }
+    }
+    if (lane == 0) { c.cnt[SPT_CNT_NEAR_PAIRS] += n_near; c.cnt[SPT_CNT_RING_NEAR] += n_ring_near; }
+    __syncthreads();
+
+    // C: far sum, rounds of kRound points over TMA-staged node tiles
+    const int segs_per_tile = kTileNodes / nps;
+    const int tile_nodes = segs_per_tile * nps;
+    const int n_tiles = (nseg + segs_per_tile - 1) / segs_per_tile;
+    double* tile[2] = {c.tiles, c.tiles + 3 * kTileNodes};
+    uint64_t* bars = c.bars;
+    unsigned long long far_evals = 0;
+    for (int r0 = 0; r0 < n; r0 += kRound) {
+        const int np_ = min(kRound, n - r0);
+        double pr[kRound], pz[kRound], ar[kRound], az[kRound];
+#pragma unroll
+        for (int p = 0; p < kRound; ++p) {
+            const int k = r0 + (p < np_ ? p : 0);
+            pr[p] = P[8 * k + 3];
+            pz[p] = P[8 * k + 4];
+            ar[p] = 0.0;
+            az[p] = 0.0;
+        }
+        uint32_t phase[2] = {0, 0};
+        auto issue = [&](int t, int buf) {
+            const int s_first = t * segs_per_tile;
+            const int nn = min(segs_per_tile, nseg - s_first) * nps;
+            const uint32_t bytes = (uint32_t)nn * 8u;
+            mbar_expect_tx(&bars[buf], 3u * bytes);
+            for (int row = 0; row < 3; ++row)
+                tma_load_1d(tile[buf] + row * kTileNodes, b.node + (size_t)row * b.node_stride + (size_t)s_first * nps,
+                            bytes, &bars[buf]);
+        };
+        if (tid == 0) {
+            issue(0, 0);
+            if (n_tiles > 1) issue(1, 1);
+        }
+        bool ok = true;
+        for (int t = 0; t < n_tiles; ++t) {
+            const int buf = t & 1;
+            const int s_first = t * segs_per_tile;
+            const int ns = min(segs_per_tile, nseg - s_first);
+            // near flags for (point, segment) of this tile
+            for (int idx = tid; idx < np_ * ns; idx += kThreads) {
+                const int p = idx / ns, sl = idx - p * ns;
+                double proj, dist;
+                c.nflag[p * 256 + sl] = seg_near(b, s_first + sl, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4], proj, dist);
+            }
+            if (!mbar_wait(&bars[buf], phase[buf])) ok = false;
+            phase[buf] ^= 1u;
+            __syncthreads();
+            if (ok) {
+                const double* tr = tile[buf];
+                const double* tz = tr + kTileNodes;
+                const double* tw = tz + kTileNodes;
+                const int nn = ns * nps;
+                for (int qn = tid; qn < nn; qn += kThreads) {
+                    const int sl = qn / nps;
+                    const double rq = tr[qn], zq = tz[qn], wq = tw[qn];
+#pragma unroll
+                    for (int p = 0; p < kRound; ++p) {
+                        if (p < np_ && !c.nflag[p * 256 + sl]) {
+                            double er, ez;
+                            ring_field(pr[p], pz[p] - zq, rq, er, ez);
+                            ar[p] = fma(wq, er, ar[p]);
+                            az[p] = fma(wq, ez, az[p]);
+                            ++far_evals;
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if (tid == 0 && t + 2 < n_tiles) issue(t + 2, buf);
+        }
+        if (!ok && tid == 0) *status_flag = SPT_GROUP_TIMEOUT;
+        // fixed-order block reduction of the round's accumulators
+#pragma unroll
+        for (int p = 0; p < kRound; ++p) {
+            const double vr = warp_sum(ar[p]);
+            const double vz = warp_sum(az[p]);
+            if (lane == 0) {
+                c.red[warp * 2 * kRound + p] = vr;
+                c.red[warp * 2 * kRound + kRound + p] = vz;
+            }
+        }
+        __syncthreads();
+        if (tid < np_) {
+            double sr = 0.0, sz = 0.0;
+            for (int w = 0; w < kWarps; ++w) {
+                sr += c.red[w * 2 * kRound + tid];
+                sz += c.red[w * 2 * kRound + kRound + tid];
+            }
+            const int k = r0 + tid;
+            const double e_rho = sr + P[8 * k + 7];
+            const double e_z = sz + c.fld[3 * k + 2];
+            P[8 * k + 5] = e_rho;
+            P[8 * k + 6] = e_z;
+        }
+        __syncthreads();
+    }
+    c.cnt[SPT_CNT_RING_FAR] += far_evals;
+    // D: rotate E_rho into (x, y)
+    for (int k = tid; k < n; k += kThreads) {
+        const double x = P[8 * k + 0], y = P[8 * k + 1];
+        const double rho = hypot(x, y);
+        const double e_rho = P[8 * k + 5], e_z = P[8 * k + 6];
+        double ex = 0.0, ey = 0.0;
+        if (rho != 0.0) {
+            ex = e_rho * (x / rho);
+            ey = e_rho * (y / rho);
+        }
+        if (scatter) {
+            const int i = c.list[k];
+            c.fld[3 * i + 0] = ex;
+            c.fld[3 * i + 1] = ey;
+            c.fld[3 * i + 2] = e_z;
+        } else {
+            P[8 * k + 5] = ex;
+            P[8 * k + 6] = ey;
+            P[8 * k + 7] = e_z;
+        }
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// one stage evaluation for the CTA's group: acc = cm*E + Fc/m + Fimg/m on
+// live particles (geometry.py:289-299).  Positions in c.sp (3E), result in
+// out (3 arrays of stride E... stored as out[0*E+i], out[E+i], out[2E+i]).
+
+template <int KIND>
+__device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
+    const int E = c.E, tid = threadIdx.x;
+    const double* sx = c.sp;
+    const double* sy = c.sp + E;
+    const double* sz = c.sp + 2 * E;
+    const SptGeometry& g = c.g;
+
+    // 1. external field
+    if (KIND == SPT_GEOM_TIP_BEM || KIND == SPT_GEOM_WELL_BEM || KIND == SPT_GEOM_POST_BEM) {
+        // compact the particles that need the BEM sum into c.list (stable order)
+        __shared__ int s_wcount[kWarps + 1];
+        int n_list = 0;
+        for (int base = 0; base < E; base += kThreads) {
+            const int i = base + tid;
+            bool need = false;
+            if (i < E && c.live[i]) {
+                const double x = sx[i], y = sy[i], z = sz[i];
+                need = bem_valid<KIND>(x, y, z, g) && blend_weight(z, g.z_handoff) > 0.0;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, need);
+            if ((tid & 31) == 0) s_wcount[tid >> 5] = __popc(bal);
+            __syncthreads();
+            if (tid == 0) {
+                int acc = 0;
+                for (int w = 0; w < kWarps; ++w) { const int t = s_wcount[w]; s_wcount[w] = acc; acc += t; }
+                s_wcount[kWarps] = acc;
+            }
+            __syncthreads();
+            if (need) {
+                const int pos = n_list + s_wcount[tid >> 5] + __popc(bal & ((1u << (tid & 31)) - 1u));
+                c.list[pos] = i;
+                c.bpt[8 * pos + 0] = sx[i];
+                c.bpt[8 * pos + 1] = sy[i];
+                c.bpt[8 * pos + 2] = sz[i];
+            }
+            n_list += s_wcount[kWarps];
+            __syncthreads();
+        }
+        if (n_list > 0) bem_points(c, n_list, false, status_flag);
+        // scatter: fld[i] = blended field
+        for (int i = tid; i < E; i += kThreads) { c.fld[3 * i + 0] = 0.0; c.fld[3 * i + 1] = 0.0; c.fld[3 * i + 2] = 0.0; }
+        __syncthreads();
+        for (int k = tid; k < n_list; k += kThreads) {
+            const int i = c.list[k];
+            c.fld[3 * i + 0] = c.bpt[8 * k + 5];
+            c.fld[3 * i + 1] = c.bpt[8 * k + 6];
+            c.fld[3 * i + 2] = c.bpt[8 * k + 7];
+        }
+        __syncthreads();
+    }
+
+    // 2. image sources for the sphere-on-plane construction (forces.py:170-183)
+    const bool three_img = (KIND == SPT_GEOM_TIP || KIND == SPT_GEOM_POST_BEM) && g.has_image;
+    if (three_img) {
+        const double a = g.R - g.z0;
+        const double zc = (KIND == SPT_GEOM_POST_BEM) ? g.L : 0.0;
+        for (int j = tid; j < E; j += kThreads) {
+            const double x = sx[j], y = sy[j], z = sz[j] - zc;
+            const double d = sqrt(x * x + y * y + z * z);
+            const double ds = d > 0.0 ? d : a;
+            const double sh = (a * a) / (ds * ds);
+            c.img[j] = x * sh;
+            c.img[E + j] = y * sh;
+            c.img[2 * E + j] = z * sh;
+            c.img[3 * E + j] = -c.q[j] * (a / ds);
+        }
+        __syncthreads();
+    }
+
+    // 3. per particle: field + pair sums
+    unsigned long long pairs = 0;
+    for (int i = tid; i < E; i += kThreads) {
+        double ax = 0.0, ay = 0.0, az = 0.0;
+        if (c.live[i]) {
+            const double xi = sx[i], yi = sy[i], zi = sz[i];
+            double ex, ey, ez;
+            if (KIND == SPT_GEOM_FLAT) {
+                ex = 0.0; ey = 0.0; ez = (zi >= 0.0) ? g.E_gun : 0.0;
+            } else if (KIND == SPT_GEOM_TIP) {
+                tip_field(xi, yi, zi, g.E_gun, g.R, ex, ey, ez);
+            } else {
+                // blend(near, far) with near = where(valid, uniform + pert, 0) (bem/geometry.py:44-55, bem/fields.py:186-211)
+                const double w = blend_weight(zi, g.z_handoff);
+                const bool valid = bem_valid<KIND>(xi, yi, zi, g);
+                const double fz = (zi >= 0.0) ? g.E_gun : 0.0;
+                double nx = 0.0, ny = 0.0, nz = 0.0;
+                if (valid && w > 0.0) {
+                    nx = 0.0 + c.fld[3 * i + 0];
+                    ny = 0.0 + c.fld[3 * i + 1];
+                    nz = g.E_gun + c.fld[3 * i + 2];
+                } else if (valid) {
+                    nx = 0.0; ny = 0.0; nz = g.E_gun;  // pert finite; times w = 0
+                }
+                ex = w * nx + (1.0 - w) * 0.0;
+                ey = w * ny + (1.0 - w) * 0.0;
+                ez = w * nz + (1.0 - w) * fz;
+            }
+            const double qk = c.kc * c.q[i];
+            double fcx = 0.0, fcy = 0.0, fcz = 0.0;
+            if (E > 1) {
+                for (int j = 0; j < E; ++j) {
+                    if (!c.live[j]) continue;
+                    const double dx = xi - sx[j], dy = yi - sy[j], dz = zi - sz[j];
+                    const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
+                    const double r3 = r2 * sqrt(r2);
+                    const double cf = qk * c.q[j] / r3;
+                    fcx = fma(cf, dx, fcx);
+                    fcy = fma(cf, dy, fcy);
+                    fcz = fma(cf, dz, fcz);
+                }
+                pairs += E;
+            }
+            double fix = 0.0, fiy = 0.0, fiz = 0.0;
+            if (KIND == SPT_GEOM_FLAT && g.has_image) {
+                const double zimg = -2.0 * g.z0;
+                for (int j = 0; j < E; ++j) {
+                    if (!c.live[j]) continue;
+                    const double dx = xi - sx[j], dy = yi - sy[j], dz = zi - (zimg - sz[j]);
+                    const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
+                    const double r3 = r2 * sqrt(r2);
+                    const double cf = qk * (-c.q[j]) / r3;
+                    fix = fma(cf, dx, fix);
+                    fiy = fma(cf, dy, fiy);
+                    fiz = fma(cf, dz, fiz);
+                }
+                pairs += E;
+            } else if (three_img) {
+                const double zc = (KIND == SPT_GEOM_POST_BEM) ? g.L : 0.0;
+                const double pz0 = (KIND == SPT_GEOM_POST_BEM) ? g.L + g.z0 : g.z0;
+                const double zl = zi - zc;
+                double s1x = 0, s1y = 0, s1z = 0, s2x = 0, s2y = 0, s2z = 0, s3x = 0, s3y = 0, s3z = 0;
+                for (int j = 0; j < E; ++j) {
+                    if (!c.live[j]) continue;
+                    const double qj = c.q[j];
+                    const double ix = c.img[j], iy = c.img[E + j], iz = c.img[2 * E + j], iq = c.img[3 * E + j];
+                    {   // sphere image
+                        const double dx = xi - ix, dy = yi - iy, dz = zl - iz;
+                        const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
+                        const double cf = qk * iq / (r2 * sqrt(r2));
+                        s1x = fma(cf, dx, s1x); s1y = fma(cf, dy, s1y); s1z = fma(cf, dz, s1z);
+                    }
+                    {   // plane image
+                        const double dx = xi - sx[j], dy = yi - sy[j], dz = zl - (-2.0 * pz0 - (sz[j] - zc));
+                        const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
+                        const double cf = qk * (-qj) / (r2 * sqrt(r2));
+                        s2x = fma(cf, dx, s2x); s2y = fma(cf, dy, s2y); s2z = fma(cf, dz, s2z);
+                    }
+                    {   // plane image of the sphere image
+                        const double dx = xi - ix, dy = yi - iy, dz = zl - (-2.0 * pz0 - iz);
+                        const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
+                        const double cf = qk * (-iq) / (r2 * sqrt(r2));
+                        s3x = fma(cf, dx, s3x); s3y = fma(cf, dy, s3y); s3z = fma(cf, dz, s3z);
+                    }
+                }
+                fix = (s1x + s2x) + s3x;
+                fiy = (s1y + s2y) + s3y;
+                fiz = (s1z + s2z) + s3z;
+                pairs += 3 * E;
+            }
+            const double mi = c.m[i];
+            ax = (c.cm * ex + fcx / mi) + fix / mi;
+            ay = (c.cm * ey + fcy / mi) + fiy / mi;
+            az = (c.cm * ez + fcz / mi) + fiz / mi;
+        }
+        out[i] = ax;
+        out[E + i] = ay;
+        out[2 * E + i] = az;
+    }
+    c.cnt[SPT_CNT_PAIR_EVALS] += pairs;
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// flush per-thread counters (all threads call)
+__device__ inline void flush_counters(Ctx& c, unsigned long long* counters) {
+    if (!counters) return;
+    for (int k = 0; k < SPT_N_COUNTERS; ++k) {
+        unsigned long long v = c.cnt[k];
+        v = warp_sum(v);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(counters + k, v);
+        c.cnt[k] = 0;
+    }
+}
+
+__device__ inline void init_barriers(Ctx& c) {
+    if (threadIdx.x == 0) {
+        mbar_init(&c.bars[0], 1);
+        mbar_init(&c.bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// the persistent integrator
+
+struct GroupScalars {
+    double t, h, hr, next_cp, err, h_next;
+    int status, exhausted, accepted;
+    long long n_acc, n_rej;
+};
+
+template <int KIND>
+__global__ void __launch_bounds__(kThreads, 1)
+trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* work, double* big_slots) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ GroupScalars gs;
+    __shared__ int s_g;
+    __shared__ double s_red[kWarps];
+    __shared__ int s_flag;
+    const int tid = threadIdx.x;
+    Ctx c;
+    c.g = geo;
+    c.bem = bem;
+    c.cm = prm.charge_to_mass;
+    c.kc = prm.coulomb_constant;
+    c.soft2 = prm.plummer_radius * prm.plummer_radius;
+    c.form = prm.form;
+    const int Emax = st.max_group_size;
+    bind(c, smem, Emax, big_slots ? big_slots + (size_t)blockIdx.x * big_slot_doubles(Emax) : nullptr);
+    init_barriers(c);
+
+    for (;;) {
+        if (tid == 0) s_g = atomicAdd(work, 1);
+        __syncthreads();
+        const int gi = s_g;
+        __syncthreads();
+        if (gi >= st.n_groups) break;
+        const int g = st.group_order ? st.group_order[gi] : gi;
+        const long long base = st.group_offset[g];
+        const int E = (int)(st.group_offset[g + 1] - base);
+        if (tid == 0) {
+            gs.status = st.status[g];
+            gs.t = st.t[g];
+            gs.h = st.h[g];
+            gs.n_acc = st.n_accepted[g];
+            gs.n_rej = st.n_rejected[g];
+            s_flag = 0;
+        }
+        __syncthreads();
+        if (E <= 0 || gs.status >= SPT_GROUP_DONE) continue;
+        // rebind with this group's size (layout offsets depend on E only through Emax; keep Emax layout)
+        c.E = E;
+        double* y0[6]; double* nw[6];
+        for (int k = 0; k < 6; ++k) { y0[k] = c.y0 + k * Emax; nw[k] = c.nw + k * Emax; }
+        for (int i = tid; i < E; i += kThreads) {
+            y0[0][i] = st.x[base + i]; y0[1][i] = st.y[base + i]; y0[2][i] = st.z[base + i];
+            y0[3][i] = st.vx[base + i]; y0[4][i] = st.vy[base + i]; y0[5][i] = st.vz[base + i];
+            c.tb[i] = st.t_birth[base + i];
+            c.td[i] = st.t_death[base + i];
+            c.q[i] = st.charge[base + i];
+            c.m[i] = st.mass[base + i];
+        }
+        __syncthreads();
+        // sorted birth times (batched_rk45.py:164): rank sort, ties by index
+        for (int i = tid; i < E; i += kThreads) {
+            const double v = c.tb[i];
+            int r = 0;
+            for (int j = 0; j < E; ++j) { const double u = c.tb[j]; r += (u < v) || (u == v && j < i); }
+            c.cps[r] = v;
+        }
+        __syncthreads();
+        if (tid == 0 && gs.status == SPT_GROUP_NEW) {
+            gs.t = c.cps[0];
+            gs.h = (prm.t_max - gs.t) * prm.initial_step_fraction;
+            gs.status = SPT_GROUP_RUNNING;
+        }
+        __syncthreads();
+        double* kp[7]; double* kv[7];
+        for (int s = 0; s < 7; ++s) { kp[s] = c.kp + 3 * s * Emax; kv[s] = c.kv + 3 * s * Emax; }
+        // The stage routines index slope arrays as out[comp*E + i] with the group's E.
+        for (long long att = 0; att < prm.max_attempts; ++att) {
+            if (gs.status != SPT_GROUP_RUNNING) break;
+            if (tid == 0) {
+                // next checkpoint (batched_rk45.py:228-242)
+                int lo = 0, hi = E;
+                while (lo < hi) { const int mid = (lo + hi) >> 1; if (c.cps[mid] <= gs.t) lo = mid + 1; else hi = mid; }
+                gs.exhausted = lo >= E;
+                gs.next_cp = gs.exhausted ? prm.t_max : c.cps[lo];
+                const double target = fmin(gs.next_cp, prm.t_max);
+                gs.hr = fmin(gs.h, target - gs.t);
+            }
+            __syncthreads();
+            const double t = gs.t, hr = gs.hr;
+            for (int i = tid; i < E; i += kThreads) c.live[i] = (t >= c.tb[i]) && (t < c.td[i]);
+            __syncthreads();
+            for (int s = 0; s < 6; ++s) {
+                for (int i = tid; i < E; i += kThreads) {
+                    double p[6];
+                    for (int k = 0; k < 6; ++k) p[k] = y0[k][i];
+                    for (int j = 0; j < s; ++j) {
+                        const double a = kA[s][j];
+                        if (a == 0.0) continue;
+                        const double ha = __dmul_rn(hr, a);
+                        for (int k = 0; k < 3; ++k) {
+                            p[k] = __dadd_rn(p[k], __dmul_rn(ha, kp[j][k * E + i]));
+                            p[3 + k] = __dadd_rn(p[3 + k], __dmul_rn(ha, kv[j][k * E + i]));
+                        }
+                    }
+                    const bool lv = c.live[i];
+                    for (int k = 0; k < 3; ++k) {
+                        c.sp[k * E + i] = p[k];
+                        kp[s][k * E + i] = lv ? p[3 + k] : 0.0;
+                    }
+                }
+                __syncthreads();
+                stage_accel<KIND>(c, kv[s], &s_flag);
+            }
+            // 5th-order solution and the endpoint stage (batched_rk45.py:365-370)
+            for (int i = tid; i < E; i += kThreads) {
+                for (int k = 0; k < 3; ++k) {
+                    double sp = 0.0, sv = 0.0;
+                    for (int j = 0; j < 6; ++j) {
+                        sp = __dadd_rn(sp, __dmul_rn(kB[j], kp[j][k * E + i]));
+                        sv = __dadd_rn(sv, __dmul_rn(kB[j], kv[j][k * E + i]));
+                    }
+                    const double pn = __dadd_rn(y0[k][i], __dmul_rn(hr, sp));
+                    const double vn = __dadd_rn(y0[3 + k][i], __dmul_rn(hr, sv));
+                    nw[k][i] = pn;
+                    nw[3 + k][i] = vn;
+                    c.sp[k * E + i] = pn;
+                    kp[6][k * E + i] = c.live[i] ? vn : 0.0;
+                }
+            }
+            __syncthreads();
+            stage_accel<KIND>(c, kv[6], &s_flag);
+            // embedded error norm (batched_rk45.py:372-393)
+            double part = 0.0;
+            for (int i = tid; i < E; i += kThreads) {
+                for (int k = 0; k < 3; ++k) {
+                    double ep = 0.0, ev = 0.0;
+                    for (int j = 0; j < 7; ++j) {
+                        ep = __dadd_rn(ep, __dmul_rn(kE[j], kp[j][k * E + i]));
+                        ev = __dadd_rn(ev, __dmul_rn(kE[j], kv[j][k * E + i]));
+                    }
+                    ep = __dmul_rn(hr, ep);
+                    ev = __dmul_rn(hr, ev);
+                    const double scp = __dadd_rn(prm.atol, __dmul_rn(prm.rtol, fmax(fabs(y0[k][i]), fabs(nw[k][i]))));
+                    const double scv = __dadd_rn(kSpeedOfLight * prm.atol,
+                                                 __dmul_rn(prm.rtol, fmax(fabs(y0[3 + k][i]), fabs(nw[3 + k][i]))));
+                    const double a = __ddiv_rn(ep, scp), b = __ddiv_rn(ev, scv);
+                    part = __dadd_rn(part, __dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+                }
+            }
+            part = warp_sum(part);
+            if ((tid & 31) == 0) s_red[tid >> 5] = part;
+            __syncthreads();
+            if (tid == 0) {
+                double sq = 0.0;
+                for (int w = 0; w < kWarps; ++w) sq += s_red[w];
+                double err = sqrt(sq / (double)(6 * E));
+                if (err == 0.0) err = kTiny;
+                const bool acc = err <= 1.0;
+                double fac = prm.safety * pow(err, -1.0 / 5.0);
+                fac = fmin(fmax(fac, prm.min_factor), prm.max_factor);
+                gs.err = err;
+                gs.accepted = acc;
+                gs.h_next = hr * fac;
+                const long long k_att = gs.n_acc + gs.n_rej;
+                if (prm.log_capacity > 0 && k_att < prm.log_capacity) {
+                    prm.log_h[(size_t)g * prm.log_capacity + k_att] = hr;
+                    prm.log_err[(size_t)g * prm.log_capacity + k_att] = err;
+                }
+                c.cnt[SPT_CNT_ATTEMPTS] += 1;
+                c.cnt[SPT_CNT_STAGE_EVALS] += 7ull * E;
+            }
+            __syncthreads();
+            if (gs.accepted) {
+                const double t_new = t + hr;
+                for (int i = tid; i < E; i += kThreads) {
+                    const bool was = c.live[i];
+                    for (int k = 0; k < 6; ++k) y0[k][i] = nw[k][i];
+                    if (was && kill_test<KIND>(nw[0][i], nw[1][i], nw[2][i], geo)) c.td[i] = t_new;
+                }
+                if (tid == 0) {
+                    gs.t = t_new;
+                    gs.n_acc += 1;
+                    const double tol = 1e-9 * fmax(prm.t_max, 1e-30);
+                    if (!gs.exhausted && t_new >= gs.next_cp - tol)
+                        gs.h = (prm.t_max - t_new) * prm.initial_step_fraction;
+                    else
+                        gs.h = gs.h_next;
+                    if (!(t_new < prm.t_max * (1 - 1e-14))) gs.status = SPT_GROUP_DONE;
+                    c.cnt[SPT_CNT_ACCEPTED] += 1;
+                    c.cnt[SPT_CNT_PARTICLE_STEPS] += (unsigned long long)E;
+                }
+            } else if (tid == 0) {
+                gs.h = gs.h_next;
+                gs.n_rej += 1;
+            }
+            if (tid == 0) {
+                if (isnan(gs.err)) gs.status = SPT_GROUP_NONFINITE;
+                if (s_flag) gs.status = s_flag;
+            }
+            __syncthreads();
+        }
+        // write back
+        for (int i = tid; i < E; i += kThreads) {
+            st.x[base + i] = y0[0][i]; st.y[base + i] = y0[1][i]; st.z[base + i] = y0[2][i];
+            st.vx[base + i] = y0[3][i]; st.vy[base + i] = y0[4][i]; st.vz[base + i] = y0[5][i];
+            st.t_death[base + i] = c.td[i];
+        }
+        if (tid == 0) {
+            st.t[g] = gs.t;
+            st.h[g] = gs.h;
+            st.status[g] = gs.status;
+            st.n_accepted[g] = gs.n_acc;
+            st.n_rejected[g] = gs.n_rej;
+        }
+        flush_counters(c, prm.counters);
+        __syncthreads();
+    }
+}
+
+// one stage evaluation per group (spt_accel)
+template <int KIND>
+__global__ void __launch_bounds__(kThreads, 1)
+accel_kernel(SptAccelArgs a, SptGeometry geo, SptBem bem) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int s_flag;
+    const int tid = threadIdx.x;
+    const int g = blockIdx.x;
+    Ctx c;
+    c.g = geo;
+    c.bem = bem;
+    c.cm = a.charge_to_mass;
+    c.kc = a.coulomb_constant;
+    c.soft2 = a.plummer_radius * a.plummer_radius;
+    c.form = a.form;
+    const int Emax = a.max_group_size;
+    // the accel path keeps no slopes: bind a layout without the big-slot region
+    bind(c, smem, Emax, nullptr);
+    init_barriers(c);
+    const long long base = a.group_offset[g];
+    const int E = (int)(a.group_offset[g + 1] - base);
+    c.E = E;
+    if (tid == 0) s_flag = 0;
+    for (int i = tid; i < E; i += kThreads) {
+        c.sp[i] = a.x[base + i];
+        c.sp[E + i] = a.y[base + i];
+        c.sp[2 * E + i] = a.z[base + i];
+        c.live[i] = a.active[base + i];
+        c.q[i] = a.charge[base + i];
+        c.m[i] = a.mass[base + i];
+    }
+    __syncthreads();
+    double* out = c.kv;  // slope storage is free on this path (groups here are at most kSmallGroup)
+    stage_accel<KIND>(c, out, &s_flag);
+    for (int i = tid; i < E; i += kThreads) {
+        a.ax[base + i] = out[i];
+        a.ay[base + i] = out[E + i];
+        a.az[base + i] = out[2 * E + i];
+    }
+}
+
+// BEM perturbation field at arbitrary points (spt_bem_field): kRound*8 points per CTA
+constexpr int kFieldChunk = 64;
+__global__ void __launch_bounds__(kThreads, 1)
+bem_field_kernel(const double* x, const double* y, const double* z, long long n, SptBem bem, double* ex, double* ey,
+                 double* ez, unsigned long long* counters) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int s_flag;
+    Ctx c;
+    c.bem = bem;
+    bind(c, smem, kFieldChunk, nullptr);
+    init_barriers(c);
+    const long long p0 = (long long)blockIdx.x * kFieldChunk;
+    const int np_ = (int)min((long long)kFieldChunk, n - p0);
+    for (int k = threadIdx.x; k < np_; k += kThreads) {
+        c.bpt[8 * k + 0] = x[p0 + k];
+        c.bpt[8 * k + 1] = y[p0 + k];
+        c.bpt[8 * k + 2] = z[p0 + k];
+    }
+    if (threadIdx.x == 0) s_flag = 0;
+    __syncthreads();
+    bem_points(c, np_, false, &s_flag);
+    for (int k = threadIdx.x; k < np_; k += kThreads) {
+        ex[p0 + k] = c.bpt[8 * k + 5];
+        ey[p0 + k] = c.bpt[8 * k + 6];
+        ez[p0 + k] = c.bpt[8 * k + 7];
+    }
+    flush_counters(c, counters);
+}
+
+__global__ void ring_kernel(const double* rho, const double* z, const double* a, long long n, int form, double* er,
+                            double* ez) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (form == SPT_FORM_FP64) {
+            ring_field(rho[i], z[i], a[i], er[i], ez[i]);
+        } else {
+            float r, zz;
+            ring_field_f((float)rho[i], (float)z[i], (float)a[i], r, zz);
+            er[i] = r;
+            ez[i] = zz;
+        }
+    }
+}
+
+__global__ void ellip_kernel(const double* p, long long n, int form, double* K, double* E) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        if (form == SPT_FORM_FP64) {
+            ellip_ke(p[i], K[i], E[i]);
+        } else {
+            float k, e;
+            ellip_ke_f((float)p[i], k, e);
+            K[i] = k;
+            E[i] = e;
+        }
+    }
+}
+
+
+// ---------------------------------------------------------------------------
+// BEM collocation matrix (AxisymmetricBEMSolution.solve, bem/axisymmetric.py:411-443
+// with the adaptive segment rule of :275-302): A[i][j] is the potential at
+// profile node i of the P1 hat density of node j.  One thread per (node i,
+// segment j) pair walks the bisection tree depth first with an explicit
+// stack (refine while length > refine_ratio * distance to the sub-segment
+// midpoint, up to max_depth), Gauss-4 on each leaf, and adds the two hat
+// halves into A[i][j] and A[i][j+1] with atomics (the two segments adjacent
+// to node j both contribute to column j).
+__device__ __forceinline__ double ring_potential(double rho, double z, double a) {
+    const double D = (rho + a) * (rho + a) + z * z;
+    const double p = ((rho - a) * (rho - a) + z * z) / D;
+    double K, E;
+    ellip_ke(p, K, E);
+    return K / (2.0 * kPi * kPi * sqrt(D));
+}
+
+__global__ void assemble_kernel(const double* pr, const double* pz, int n, double refine_ratio, int max_depth,
+                                const double* g4x, const double* g4w, double* A) {
+    const long long pair = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long n_pairs = (long long)n * (n - 1);
+    if (pair >= n_pairs) return;
+    const int i = (int)(pair / (n - 1));
+    const int j = (int)(pair - (long long)i * (n - 1));
+    const double rf = pr[i], zf = pz[i];
+    // stack entries: t0, t1 (parameters along segment j), depth
+    double st0[48], st1[48];
+    int sd[48];
+    int top = 0;
+    st0[0] = 0.0; st1[0] = 1.0; sd[0] = 0; top = 1;
+    const double ar = pr[j], az = pz[j], br = pr[j + 1], bz = pz[j + 1];
+    double acc0 = 0.0, acc1 = 0.0;  // hat of node j (1 -> 0) and of node j+1 (0 -> 1)
+    while (top > 0) {
+        --top;
+        const double t0 = st0[top], t1 = st1[top];
+        const int depth = sd[top];
+        const double p0r = ar + t0 * (br - ar), p0z = az + t0 * (bz - az);
+        const double p1r = ar + t1 * (br - ar), p1z = az + t1 * (bz - az);
+        const double mr = 0.5 * (p0r + p1r), mz = 0.5 * (p0z + p1z);
+        const double len = sqrt((p1r - p0r) * (p1r - p0r) + (p1z - p0z) * (p1z - p0z));
+        const double dist = sqrt((rf - mr) * (rf - mr) + (zf - mz) * (zf - mz));
+        if (depth < max_depth && len > refine_ratio * dist && top + 2 <= 48) {
+            const double tm = 0.5 * (t0 + t1);
+            st0[top] = tm; st1[top] = t1; sd[top] = depth + 1; ++top;   // right half, processed second
+            st0[top] = t0; st1[top] = tm; sd[top] = depth + 1; ++top;   // left half first
+            continue;
+        }
+        for (int k = 0; k < 4; ++k) {
+            const double u = 0.5 * (g4x[k] + 1.0);
+            const double rs = p0r + u * (p1r - p0r), zs = p0z + u * (p1z - p0z);
+            const double tt = t0 + u * (t1 - t0);          // position along the full segment
+            const double base = 2.0 * kPi * rs * ring_potential(rf, zf - zs, rs) * (len * 0.5 * g4w[k]);
+            acc0 += (1.0 - tt) * base;
+            acc1 += tt * base;
+        }
+    }
+    atomicAdd(&A[(size_t)i * n + j], acc0);
+    atomicAdd(&A[(size_t)i * n + j + 1], acc1);
+}
+
+}  // namespace spt
+
+// ===========================================================================
+// C ABI
+
+namespace {
+thread_local char g_err[512];
+
+int fail(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_check(cudaError_t e, const char* what) {
+    if (e != cudaSuccess) return fail(SPT_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return SPT_OK;
+}
+
+int check_bem(const SptBem* b) {
+    if (!b || !b->seg || !b->node) return fail(SPT_ERR_ARG, "BEM tables required for this geometry");
+    if (b->n_seg <= 0 || b->nodes_per_seg <= 0 || b->nodes_per_seg % 4 || b->nodes_per_seg > spt::kTileNodes)
+        return fail(SPT_ERR_ARG, "nodes_per_seg must be a positive multiple of 4, at most %d", spt::kTileNodes);
+    if ((reinterpret_cast<uintptr_t>(b->node) & 15) || (b->node_stride & 1))
+        return fail(SPT_ERR_ARG, "node table must be 16-byte aligned with an even row stride");
+    if (b->node_stride < (int64_t)b->n_seg * b->nodes_per_seg || b->seg_stride < b->n_seg)
+        return fail(SPT_ERR_ARG, "table strides too small");
+    return SPT_OK;
+}
+
+bool is_bem(int kind) { return kind == SPT_GEOM_TIP_BEM || kind == SPT_GEOM_WELL_BEM || kind == SPT_GEOM_POST_BEM; }
+
+template <typename K>
+int set_smem(K kernel, size_t bytes) {
+    return cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
+                      "cudaFuncSetAttribute");
+}
+
+int grid_for(int n_groups, int blocks_per_sm_hint) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long cap = (long long)sms * blocks_per_sm_hint;
+    return (int)(n_groups < cap ? n_groups : cap);
+}
+
+template <int KIND>
+int launch_trace(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b, void* ws,
+                 int64_t ws_bytes, cudaStream_t stream) {
+    const spt::Layout L = spt::make_layout(s->max_group_size, true);
+    auto kern = spt::trace_kernel<KIND>;
+    int rc = set_smem(kern, L.bytes);
+    if (rc) return rc;
+    int per_sm = 0;
+    rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, spt::kThreads, L.bytes), "occupancy");
+    if (rc) return rc;
+    if (per_sm < 1) return fail(SPT_ERR_CAPACITY, "group size %d does not fit one CTA", s->max_group_size);
+    const int grid = grid_for(s->n_groups, per_sm);
+    int* work = static_cast<int*>(ws);
+    double* slots = nullptr;
+    if (L.big) slots = reinterpret_cast<double*>(static_cast<char*>(ws) + 256);
+    const int64_t need = 256 + (L.big ? (int64_t)grid * (int64_t)spt::big_slot_doubles(s->max_group_size) * 8 : 0);
+    if (ws_bytes < need) return fail(SPT_ERR_ARG, "workspace too small: %lld < %lld", (long long)ws_bytes, (long long)need);
+    rc = cuda_check(cudaMemsetAsync(work, 0, sizeof(int), stream), "cudaMemsetAsync");
+    if (rc) return rc;
+    SptBem bem = b ? *b : SptBem{};
+    kern<<<grid, spt::kThreads, L.bytes, stream>>>(*s, *p, *g, bem, work, slots);
+    return cuda_check(cudaGetLastError(), "trace_kernel launch");
+}
+
+}  // namespace
+
+extern "C" {
+
+int spt_abi_version(void) { return SPT_ABI_VERSION; }
+
+int spt_last_error(char* buf, int32_t len) {
+    const int n = (int)strlen(g_err);
+    if (buf && len > 0) {
+        strncpy(buf, g_err, len - 1);
+        buf[len - 1] = 0;
+    }
+    return n;
+}
+
+int spt_trace_workspace_bytes(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b,
+                              int64_t* bytes) {
+    (void)p; (void)g; (void)b;
+    if (!s || !bytes) return fail(SPT_ERR_ARG, "null argument");
+    const spt::Layout L = spt::make_layout(s->max_group_size, true);
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int64_t n = 256;
+    if (L.big) n += (int64_t)sms * 2 * (int64_t)spt::big_slot_doubles(s->max_group_size) * 8;
+    *bytes = n;
+    return SPT_OK;
+}
+
+int spt_trace(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b, void* ws,
+              int64_t ws_bytes, void* stream) {
+    if (!s || !p || !g || !ws) return fail(SPT_ERR_ARG, "null argument");
+    if (s->n_groups <= 0) return SPT_OK;
+    if (s->max_group_size <= 0 || s->max_group_size > 1024)
+        return fail(SPT_ERR_CAPACITY, "max_group_size %d outside [1, 1024]", s->max_group_size);
+    if (reinterpret_cast<uintptr_t>(ws) & 255) return fail(SPT_ERR_ARG, "workspace must be 256-byte aligned");
+    if (p->form != SPT_FORM_FP64 && p->form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "unknown form %d", p->form);
+    if (is_bem(g->kind)) {
+        const int rc = check_bem(b);
+        if (rc) return rc;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    switch (g->kind) {
+        case SPT_GEOM_FLAT: return launch_trace<SPT_GEOM_FLAT>(s, p, g, b, ws, ws_bytes, st);
+        case SPT_GEOM_TIP: return launch_trace<SPT_GEOM_TIP>(s, p, g, b, ws, ws_bytes, st);
+        case SPT_GEOM_TIP_BEM: return launch_trace<SPT_GEOM_TIP_BEM>(s, p, g, b, ws, ws_bytes, st);
+        case SPT_GEOM_WELL_BEM: return launch_trace<SPT_GEOM_WELL_BEM>(s, p, g, b, ws, ws_bytes, st);
+        case SPT_GEOM_POST_BEM: return launch_trace<SPT_GEOM_POST_BEM>(s, p, g, b, ws, ws_bytes, st);
+        default: return fail(SPT_ERR_ARG, "unknown geometry kind %d", g->kind);
+    }
+}
+
+int spt_accel(const SptAccelArgs* a, const SptGeometry* g, const SptBem* b, void* stream) {
+    if (!a || !g) return fail(SPT_ERR_ARG, "null argument");
+    if (a->n_groups <= 0) return SPT_OK;
+    if (a->max_group_size <= 0 || a->max_group_size > spt::kSmallGroup)
+        return fail(SPT_ERR_CAPACITY, "spt_accel: group size must be in [1, %d]", spt::kSmallGroup);
+    if (is_bem(g->kind)) {
+        const int rc = check_bem(b);
+        if (rc) return rc;
+    }
+    int rc = SPT_OK;
+    const spt::Layout L = spt::make_layout(a->max_group_size, true);
+    SptBem bem = b ? *b : SptBem{};
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+#define SPT_LAUNCH_ACCEL(K)                                                                  \
+    {                                                                                        \
+        rc = set_smem(spt::accel_kernel<K>, L.bytes);                                         \
+        if (rc) return rc;                                                                   \
+        spt::accel_kernel<K><<<a->n_groups, spt::kThreads, L.bytes, st>>>(*a, *g, bem);       \
+        return cuda_check(cudaGetLastError(), "accel_kernel launch");                       \
+    }
+    switch (g->kind) {
+        case SPT_GEOM_FLAT: SPT_LAUNCH_ACCEL(SPT_GEOM_FLAT)
+        case SPT_GEOM_TIP: SPT_LAUNCH_ACCEL(SPT_GEOM_TIP)
+        case SPT_GEOM_TIP_BEM: SPT_LAUNCH_ACCEL(SPT_GEOM_TIP_BEM)
+        case SPT_GEOM_WELL_BEM: SPT_LAUNCH_ACCEL(SPT_GEOM_WELL_BEM)
+        case SPT_GEOM_POST_BEM: SPT_LAUNCH_ACCEL(SPT_GEOM_POST_BEM)
+        default: return fail(SPT_ERR_ARG, "unknown geometry kind %d", g->kind);
+    }
+#undef SPT_LAUNCH_ACCEL
+}
+
+int spt_bem_field(const double* x, const double* y, const double* z, int64_t n, const SptBem* b, int32_t form,
+                  double* ex, double* ey, double* ez, void* stream) {
+    if (n <= 0) return SPT_OK;
+    if (!x || !y || !z || !ex || !ey || !ez) return fail(SPT_ERR_ARG, "null argument");
+    int rc = check_bem(b);
+    if (rc) return rc;
+    (void)form;
+    const spt::Layout L = spt::make_layout(spt::kFieldChunk, true);
+    rc = set_smem(spt::bem_field_kernel, L.bytes);
+    if (rc) return rc;
+    const long long blocks = (n + spt::kFieldChunk - 1) / spt::kFieldChunk;
+    if (blocks > 0x7fffffffLL) return fail(SPT_ERR_CAPACITY, "too many points");
+    spt::bem_field_kernel<<<(unsigned)blocks, spt::kThreads, L.bytes, static_cast<cudaStream_t>(stream)>>>(
+        x, y, z, n, *b, ex, ey, ez, nullptr);
+    return cuda_check(cudaGetLastError(), "bem_field_kernel launch");
+}
+
+int spt_ring_field(const double* rho, const double* z, const double* a, int64_t n, int32_t form, double* er,
+                   double* ez, void* stream) {
+    if (n <= 0) return SPT_OK;
+    if (!rho || !z || !a || !er || !ez) return fail(SPT_ERR_ARG, "null argument");
+    const long long blocks = (n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8;
+    spt::ring_kernel<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(rho, z, a, n, form, er, ez);
+    return cuda_check(cudaGetLastError(), "ring_kernel launch");
+}
+
+int spt_ellip_ke(const double* p, int64_t n, int32_t form, double* K, double* E, void* stream) {
+    if (n <= 0) return SPT_OK;
+    if (!p || !K || !E) return fail(SPT_ERR_ARG, "null argument");
+    const long long blocks = (n + 255) / 256 < 148 * 8 ? (n + 255) / 256 : 148 * 8;
+    spt::ellip_kernel<<<(unsigned)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(p, n, form, K, E);
+    return cuda_check(cudaGetLastError(), "ellip_kernel launch");
+}
+
+int spt_bem_assemble(const double* profile_rho, const double* profile_z, int32_t n_nodes, double refine_ratio,
+                     int32_t max_depth, const double* gauss4_x, const double* gauss4_w, double* A, void* stream) {
+    if (n_nodes < 2) return fail(SPT_ERR_ARG, "profile needs at least 2 nodes");
+    if (!profile_rho || !profile_z || !A || !gauss4_x || !gauss4_w) return fail(SPT_ERR_ARG, "null argument");
+    if (max_depth < 0 || max_depth > 40) return fail(SPT_ERR_CAPACITY, "max_depth must be in [0, 40]");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int rc = cuda_check(cudaMemsetAsync(A, 0, sizeof(double) * (size_t)n_nodes * n_nodes, st), "cudaMemsetAsync");
+    if (rc) return rc;
+    const long long pairs = (long long)n_nodes * (n_nodes - 1);
+    const long long blocks = (pairs + 127) / 128;
+    spt::assemble_kernel<<<(unsigned)blocks, 128, 0, st>>>(profile_rho, profile_z, n_nodes, refine_ratio, max_depth,
+                                                         gauss4_x, gauss4_w, A);
+    return cuda_check(cudaGetLastError(), "assemble_kernel launch");
+}
+
+}  // extern "C"

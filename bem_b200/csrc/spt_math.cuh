@@ -1,0 +1,148 @@
+// Device math for the tracer: complete elliptic integrals K(1-p), E(1-p)
+// and the unit-charge ring field, float64 and float32.
+//
+// K and E are computed here from published methods (not from SciPy's or
+// CUDA's code):
+//   * p < 1e-3 : the logarithmic series about m = 1 of DLMF 19.12.1 (K) and
+//                19.12.2 (E), in powers of p = 1 - m with L = ln(1/sqrt(p)):
+//                K = sum a_n^2 p^n (L + d_n),
+//                E = 1 + (p/2) sum b_n p^n (L + d_n - 1/((2n+1)(2n+2))),
+//                a_n = (1/2)_n/n!, b_n = (1/2)_n (3/2)_n / ((2)_n n!),
+//                d_n = psi(1+n) - psi(1/2+n) = 2 ln 2 - sum_{k<=n} 1/(k(2k-1)).
+//                Ten terms keep the truncation below 1e-29 for p < 1e-3.
+//   * p >= 1e-3: the arithmetic-geometric mean, DLMF 19.8.1 (K = pi/(2 M)) and
+//                19.8.6 (E = K (1 - sum 2^(n-1) c_n^2)), started from
+//                a0 = 1, b0 = sqrt(p), c0^2 = 1 - p.
+// Checked against SciPy's ellipkm1/ellipe to 3 ulp on p in [1e-300, 1].
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace spt {
+
+constexpr double kPi = 3.141592653589793;
+
+// Series coefficients of the two DLMF 19.12 expansions (a_n^2, a_n^2 d_n,
+// b_n, b_n (d_n - 1/((2n+1)(2n+2)))), n = 0..9, computed from the
+// recurrences a_n = a_{n-1}(n-1/2)/n, b_n = b_{n-1}(n-1/2)(n+1/2)/((n+1)n),
+// d_n = d_{n-1} - 1/(n(2n-1)), d_0 = 2 ln 2.
+__device__ __constant__ double kSerK[10] = {
+    1.0, 0.25, 0.140625, 0.09765625, 0.07476806640625, 0.0605621337890625,
+    0.050889015197753906, 0.043878793716430664, 0.03856534603983164, 0.034399336436763406};
+__device__ __constant__ double kSerKd[10] = {
+    1.3862943611198906, 0.09657359027997264, 0.030885144532484612, 0.01493760036978098,
+    0.008766312197176064, 0.0057548876844001106, 0.004064658549993974, 0.003022546550344074,
+    0.0023351571703480825, 0.0018580702734561816};
+__device__ __constant__ double kSerE[10] = {
+    1.0, 0.375, 0.234375, 0.1708984375, 0.13458251953125, 0.11103057861328125,
+    0.09450817108154297, 0.0822727382183075, 0.0728456536307931, 0.06535873922985047};
+__device__ __constant__ double kSerEd[10] = {
+    0.8862943611198906, 0.11361038541995896, 0.043662740887474356, 0.023089042834616717,
+    0.014284000626791913, 0.00970948667432989, 0.007029375927562748, 0.005324471705985524,
+    0.004172794741275812, 0.0033583368373829277};
+
+__device__ __forceinline__ double horner10(const double* c, double p) {
+    double s = c[9];
+#pragma unroll
+    for (int n = 8; n >= 0; --n) s = fma(s, p, c[n]);
+    return s;
+}
+
+// K(1-p), E(1-p), float64.
+__device__ __forceinline__ void ellip_ke(double p, double& K, double& E) {
+    if (p < 1e-3) {
+        const double L = -0.5 * log(p);
+        K = fma(L, horner10(kSerK, p), horner10(kSerKd, p));
+        E = fma(0.5 * p, fma(L, horner10(kSerE, p), horner10(kSerEd, p)), 1.0);
+        return;
+    }
+    double a = 1.0, b = sqrt(p);
+    double S = 0.5 * (1.0 - p), w = 0.5;
+#pragma unroll 1
+    for (int it = 0; it < 12; ++it) {
+        const double c = 0.5 * (a - b);
+        const double an = 0.5 * (a + b);
+        b = sqrt(a * b);
+        a = an;
+        w += w;
+        S = fma(w * c, c, S);
+        if (fabs(c) <= 1e-17 * a) break;
+    }
+    K = kPi / (2.0 * a);
+    E = K * (1.0 - S);
+}
+
+// Field (E_rho, E_z) at (rho, z) of a unit-total-charge ring of radius a at
+// height 0 (G = 1/(4 pi r) convention), float64.  The formula and the
+// near-axis Taylor branch follow bem/axisymmetric.py:248-265.
+__device__ __forceinline__ void ring_field(double rho, double z, double a, double& er, double& ez) {
+    const double z2 = z * z, a2 = a * a, rho2 = rho * rho;
+    const double D = (rho + a) * (rho + a) + z2;
+    const double d2 = (rho - a) * (rho - a) + z2;
+    if (rho2 < 1e-10 * (a2 + z2)) {
+        const double ax2 = a2 + z2;
+        const double s = sqrt(ax2);
+        const double ax15 = ax2 * s, ax25 = ax2 * ax15, ax35 = ax2 * ax25;
+        er = rho * (2.0 * z2 - a2) / (8.0 * kPi * ax25);
+        ez = z / (4.0 * kPi * ax15) + 3.0 * rho2 * z * (3.0 * a2 - 2.0 * z2) / (16.0 * kPi * ax35);
+        return;
+    }
+    double K, E;
+    ellip_ke(d2 / D, K, E);
+    const double sD = sqrt(D);
+    er = (K - (a2 - rho2 + z2) * E / d2) / (4.0 * kPi * kPi * rho * sD);
+    ez = z * E / (2.0 * kPi * kPi * sD * d2);
+}
+
+// ---------------------------------------------------------------------------
+// float32 variants (SPT_FORM_MIXED).  Same methods; the series branch is
+// used below p < 1e-2 with four terms (truncation < 1e-9), the AGM above.
+__device__ __forceinline__ void ellip_ke_f(float p, float& K, float& E) {
+    if (p < 1e-2f) {
+        const float L = -0.5f * __logf(p);
+        const float A = fmaf(fmaf(fmaf(0.09765625f, p, 0.140625f), p, 0.25f), p, 1.0f);
+        const float B = fmaf(fmaf(fmaf(0.01493760037f, p, 0.03088514453f), p, 0.09657359028f), p, 1.386294361f);
+        const float C = fmaf(fmaf(fmaf(0.1708984375f, p, 0.234375f), p, 0.375f), p, 1.0f);
+        const float D = fmaf(fmaf(fmaf(0.02308904283f, p, 0.04366274089f), p, 0.1136103854f), p, 0.8862943611f);
+        K = fmaf(L, A, B);
+        E = fmaf(0.5f * p, fmaf(L, C, D), 1.0f);
+        return;
+    }
+    float a = 1.0f, b = sqrtf(p);
+    float S = 0.5f * (1.0f - p), w = 0.5f;
+#pragma unroll 1
+    for (int it = 0; it < 8; ++it) {
+        const float c = 0.5f * (a - b);
+        const float an = 0.5f * (a + b);
+        b = sqrtf(a * b);
+        a = an;
+        w += w;
+        S = fmaf(w * c, c, S);
+        if (fabsf(c) <= 3e-8f * a) break;
+    }
+    K = 1.5707963267948966f / a;
+    E = K * (1.0f - S);
+}
+
+__device__ __forceinline__ void ring_field_f(float rho, float z, float a, float& er, float& ez) {
+    const float z2 = z * z, a2 = a * a, rho2 = rho * rho;
+    const float D = (rho + a) * (rho + a) + z2;
+    const float d2 = (rho - a) * (rho - a) + z2;
+    if (rho2 < 1e-10f * (a2 + z2)) {
+        const float ax2 = a2 + z2;
+        const float r1 = rsqrtf(ax2);
+        const float i15 = r1 / ax2, i25 = i15 / ax2, i35 = i25 / ax2;
+        er = rho * (2.0f * z2 - a2) * i25 * (1.0f / (8.0f * 3.14159265f));
+        ez = z * i15 * (1.0f / (4.0f * 3.14159265f)) + 3.0f * rho2 * z * (3.0f * a2 - 2.0f * z2) * i35 * (1.0f / (16.0f * 3.14159265f));
+        return;
+    }
+    float K, E;
+    const float invD = __frcp_rn(D);
+    ellip_ke_f(d2 * invD, K, E);
+    const float rsD = rsqrtf(D);
+    const float inv_d2 = __frcp_rn(d2);
+    er = (K - (a2 - rho2 + z2) * E * inv_d2) * rsD * __frcp_rn(rho) * (1.0f / (4.0f * 9.8696044f));
+    ez = z * E * rsD * inv_d2 * (1.0f / (2.0f * 9.8696044f));
+}
+
+}  // namespace spt

@@ -1,0 +1,268 @@
+"""Device-resident trace driver over the C ABI (spt_trace).
+
+``GroupBatch`` holds the structure-of-arrays particle state and per-group
+integrator state in torch CUDA tensors (torch is only the allocator and
+stream here; all arithmetic is in the CUDA library).  ``integrate`` is the
+drop-in for batched_rk45.integrate (batched_rk45.py:55-323): it advances
+every group with its own t and h until t >= t_max, with the same stopping
+rule, birth checkpoints, kill-after-accept and step-size controller, but as
+one persistent kernel per call instead of a Python loop with host syncs.
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .constants import COULOMB_CONSTANT
+
+DEFAULT_ATTEMPT_CHUNK = 1 << 30
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _as_dev(a, dtype, device):
+    torch = _torch()
+    if isinstance(a, torch.Tensor):
+        return a.to(device=device, dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(a), dtype=dtype, device=device)
+
+
+class GroupBatch:
+    """Flat SoA particle arrays with group offsets, plus group clocks."""
+
+    def __init__(self, pos, vel, t_birth, charge, mass, group_sizes, device="cuda", order="largest_first"):
+        torch = _torch()
+        f64 = torch.float64
+        pos = np.asarray(pos, dtype=np.float64) if not isinstance(pos, torch.Tensor) else pos
+        sizes = np.asarray(group_sizes, dtype=np.int64)
+        if np.any(sizes < 1):
+            raise ValueError("every group needs at least one particle")
+        n = int(sizes.sum())
+        if pos.shape != (n, 3):
+            raise ValueError(f"pos must be ({n}, 3) for these group sizes, got {tuple(pos.shape)}")
+        if sizes.max() > 1024:
+            raise ValueError("groups larger than 1024 particles are not supported")
+        self.device = torch.device(device)
+        self.n_groups = len(sizes)
+        self.n_particles = n
+        self.sizes = sizes
+        self.max_group_size = int(sizes.max())
+        offs = np.zeros(len(sizes) + 1, dtype=np.int64)
+        np.cumsum(sizes, out=offs[1:])
+        self.offsets_host = offs
+        d = self.device
+        self.offsets = torch.as_tensor(offs, device=d)
+        if order == "largest_first":
+            perm = np.argsort(-sizes, kind="stable").astype(np.int32)
+            self.order = torch.as_tensor(perm, device=d)
+        else:
+            self.order = None
+        p = _as_dev(pos, f64, d)
+        v = _as_dev(vel, f64, d)
+        self.x, self.y, self.z = (p[:, k].contiguous() for k in range(3))
+        self.vx, self.vy, self.vz = (v[:, k].contiguous() for k in range(3))
+        self.t_birth = _as_dev(t_birth, f64, d).reshape(-1)
+        self.charge = _as_dev(charge, f64, d).reshape(-1)
+        self.mass = _as_dev(mass, f64, d).reshape(-1)
+        self.t_death = torch.full((n,), float("inf"), dtype=f64, device=d)
+        G = self.n_groups
+        self.t = torch.zeros(G, dtype=f64, device=d)
+        self.h = torch.zeros(G, dtype=f64, device=d)
+        self.status = torch.zeros(G, dtype=torch.int32, device=d)
+        self.n_accepted = torch.zeros(G, dtype=torch.int64, device=d)
+        self.n_rejected = torch.zeros(G, dtype=torch.int64, device=d)
+
+    def struct(self):
+        s = _lib.SptState()
+        s.n_groups = self.n_groups
+        s.max_group_size = self.max_group_size
+        s.n_particles = self.n_particles
+        P = lambda t: None if t is None else t.data_ptr()
+        s.group_offset = P(self.offsets)
+        s.group_order = P(self.order)
+        s.x, s.y, s.z = P(self.x), P(self.y), P(self.z)
+        s.vx, s.vy, s.vz = P(self.vx), P(self.vy), P(self.vz)
+        s.t_birth, s.t_death = P(self.t_birth), P(self.t_death)
+        s.charge, s.mass = P(self.charge), P(self.mass)
+        s.t, s.h, s.status = P(self.t), P(self.h), P(self.status)
+        s.n_accepted, s.n_rejected = P(self.n_accepted), P(self.n_rejected)
+        return s
+
+    def positions(self):
+        torch = _torch()
+        return torch.stack([self.x, self.y, self.z], dim=-1)
+
+    def velocities(self):
+        torch = _torch()
+        return torch.stack([self.vx, self.vy, self.vz], dim=-1)
+
+
+FORMS = {"fp64": _lib.FORM_FP64, "mixed": _lib.FORM_MIXED}
+
+
+class Tracer:
+    """Persistent-kernel RK45 tracer for one geometry on one device."""
+
+    def __init__(self, geometry, device="cuda", form="fp64", z_max=None):
+        torch = _torch()
+        self.geometry = geometry
+        self.device = torch.device(device)
+        self.form = FORMS[form] if isinstance(form, str) else int(form)
+        self.z_max = z_max
+        self.geom = geometry.to_struct(z_max=z_max)
+        self.tables = geometry.bem_tables(self.device) if geometry.is_bem else None
+        self._ws = None
+        self.counters = torch.zeros(_lib.N_COUNTERS, dtype=torch.int64, device=self.device)
+
+    def params(self, t_max, rtol, atol, plummer_radius, charge_to_mass, max_attempts, log=None,
+               safety=0.9, min_factor=0.2, max_factor=10.0, initial_step_fraction=1e-6,
+               coulomb_constant=COULOMB_CONSTANT):
+        p = _lib.SptTraceParams()
+        p.t_max, p.rtol, p.atol = float(t_max), float(rtol), float(atol)
+        p.plummer_radius = float(plummer_radius)
+        p.charge_to_mass = float(charge_to_mass)
+        p.coulomb_constant = float(coulomb_constant)
+        p.safety, p.min_factor, p.max_factor = float(safety), float(min_factor), float(max_factor)
+        p.initial_step_fraction = float(initial_step_fraction)
+        p.max_attempts = int(max_attempts)
+        p.form = self.form
+        if log is not None:
+            p.log_capacity = log[0].shape[1]
+            p.log_h = log[0].data_ptr()
+            p.log_err = log[1].data_ptr()
+        p.counters = self.counters.data_ptr()
+        return p
+
+    def workspace(self, state, params):
+        torch = _torch()
+        nbytes = ctypes.c_int64(0)
+        bem = ctypes.byref(self.tables.struct) if self.tables is not None else None
+        _lib.check(_lib.lib().spt_trace_workspace_bytes(ctypes.byref(state), ctypes.byref(params),
+                                                        ctypes.byref(self.geom), bem, ctypes.byref(nbytes)),
+                   "spt_trace_workspace_bytes")
+        need = max(int(nbytes.value), 256)
+        if self._ws is None or self._ws.numel() < need:
+            self._ws = torch.empty(need, dtype=torch.uint8, device=self.device)
+        return self._ws
+
+    def launch(self, batch, params, stream=None):
+        """One spt_trace call (asynchronous on `stream`)."""
+        torch = _torch()
+        st = batch.struct()
+        ws = self.workspace(st, params)
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        bem = ctypes.byref(self.tables.struct) if self.tables is not None else None
+        _lib.check(_lib.lib().spt_trace(ctypes.byref(st), ctypes.byref(params), ctypes.byref(self.geom), bem,
+                                        ctypes.c_void_p(ws.data_ptr()), ws.numel(),
+                                        ctypes.c_void_p(stream.cuda_stream)), "spt_trace")
+
+    def run(self, batch, t_max, rtol, atol, plummer_radius, charge_to_mass, max_steps=10_000_000,
+            attempt_chunk=DEFAULT_ATTEMPT_CHUNK, log_capacity=0, **kw):
+        """Integrate every group to t_max.  Raises RuntimeError when a group
+        needs more than max_steps attempts (batched_rk45.py:320-321)."""
+        torch = _torch()
+        log = None
+        if log_capacity:
+            log = (torch.full((batch.n_groups, log_capacity), float("nan"), dtype=torch.float64, device=self.device),
+                   torch.full((batch.n_groups, log_capacity), float("nan"), dtype=torch.float64, device=self.device))
+        done_attempts = 0
+        while True:
+            chunk = min(attempt_chunk, max_steps - done_attempts)
+            if chunk <= 0:
+                raise RuntimeError(f"batched RK45 did not converge within {max_steps} steps")
+            p = self.params(t_max, rtol, atol, plummer_radius, charge_to_mass, chunk, log=log, **kw)
+            self.launch(batch, p)
+            done_attempts += chunk
+            status = batch.status.cpu().numpy()
+            bad = np.isin(status, [_lib.GROUP_NONFINITE, _lib.GROUP_TIMEOUT])
+            if np.any(bad):
+                g = int(np.nonzero(bad)[0][0])
+                raise RuntimeError(f"group {g} stopped with status {int(status[g])} "
+                                   f"({'non-finite error norm' if status[g] == _lib.GROUP_NONFINITE else 'device wait timeout'})")
+            if np.all(status == _lib.GROUP_DONE):
+                break
+        return log
+
+    def counter_dict(self):
+        c = self.counters.cpu().numpy().astype(np.uint64)
+        return {k: int(v) for k, v in zip(_lib.COUNTERS, c)}
+
+
+def accel(geometry, pos, active, charge, mass, group_sizes, charge_to_mass, plummer_radius, device="cuda",
+          form="fp64", coulomb_constant=COULOMB_CONSTANT):
+    """One stage evaluation through spt_accel; returns acc [N, 3] (torch)."""
+    torch = _torch()
+    sizes = np.asarray(group_sizes, dtype=np.int64)
+    offs = np.zeros(len(sizes) + 1, dtype=np.int64)
+    np.cumsum(sizes, out=offs[1:])
+    d = torch.device(device)
+    p = _as_dev(pos, torch.float64, d)
+    x, y, z = (p[:, k].contiguous() for k in range(3))
+    act = _as_dev(np.asarray(active, dtype=np.uint8) if not isinstance(active, torch.Tensor) else active.to(torch.uint8),
+                  torch.uint8, d)
+    q = _as_dev(charge, torch.float64, d).reshape(-1)
+    m = _as_dev(mass, torch.float64, d).reshape(-1)
+    off_t = torch.as_tensor(offs, device=d)
+    out = [torch.empty_like(x) for _ in range(3)]
+    a = _lib.SptAccelArgs()
+    a.n_groups = len(sizes)
+    a.max_group_size = int(sizes.max())
+    a.n_particles = int(offs[-1])
+    a.group_offset = off_t.data_ptr()
+    a.x, a.y, a.z = x.data_ptr(), y.data_ptr(), z.data_ptr()
+    a.active, a.charge, a.mass = act.data_ptr(), q.data_ptr(), m.data_ptr()
+    a.charge_to_mass = float(charge_to_mass)
+    a.coulomb_constant = float(coulomb_constant)
+    a.plummer_radius = float(plummer_radius)
+    a.form = FORMS[form] if isinstance(form, str) else int(form)
+    a.ax, a.ay, a.az = (o.data_ptr() for o in out)
+    geom = geometry.to_struct()
+    tables = geometry.bem_tables(d) if geometry.is_bem else None
+    stream = torch.cuda.current_stream(d)
+    _lib.check(_lib.lib().spt_accel(ctypes.byref(a), ctypes.byref(geom),
+                                    ctypes.byref(tables.struct) if tables is not None else None,
+                                    ctypes.c_void_p(stream.cuda_stream)), "spt_accel")
+    return torch.stack(out, dim=-1)
+
+
+def bem_field(tables, points, form="fp64"):
+    """Perturbation field of a BEM solution at points [N, 3] (spt_bem_field)."""
+    torch = _torch()
+    p = _as_dev(points, torch.float64, tables.seg.device).reshape(-1, 3)
+    x, y, z = (p[:, k].contiguous() for k in range(3))
+    out = [torch.empty_like(x) for _ in range(3)]
+    stream = torch.cuda.current_stream(tables.seg.device)
+    _lib.check(_lib.lib().spt_bem_field(x.data_ptr(), y.data_ptr(), z.data_ptr(), x.numel(),
+                                        ctypes.byref(tables.struct), FORMS[form] if isinstance(form, str) else form,
+                                        out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(),
+                                        ctypes.c_void_p(stream.cuda_stream)), "spt_bem_field")
+    return torch.stack(out, dim=-1)
+
+
+def ring_field(rho, z, a, form="fp64", device="cuda"):
+    torch = _torch()
+    d = torch.device(device)
+    r, zz, aa = (_as_dev(v, torch.float64, d).reshape(-1) for v in (rho, z, a))
+    er, ez = torch.empty_like(r), torch.empty_like(r)
+    stream = torch.cuda.current_stream(d)
+    _lib.check(_lib.lib().spt_ring_field(r.data_ptr(), zz.data_ptr(), aa.data_ptr(), r.numel(),
+                                         FORMS[form] if isinstance(form, str) else form, er.data_ptr(),
+                                         ez.data_ptr(), ctypes.c_void_p(stream.cuda_stream)), "spt_ring_field")
+    return er, ez
+
+
+def ellip_ke(p, form="fp64", device="cuda"):
+    torch = _torch()
+    d = torch.device(device)
+    pp = _as_dev(p, torch.float64, d).reshape(-1)
+    K, E = torch.empty_like(pp), torch.empty_like(pp)
+    stream = torch.cuda.current_stream(d)
+    _lib.check(_lib.lib().spt_ellip_ke(pp.data_ptr(), pp.numel(), FORMS[form] if isinstance(form, str) else form,
+                                       K.data_ptr(), E.data_ptr(), ctypes.c_void_p(stream.cuda_stream)),
+               "spt_ellip_ke")
+    return K, E

@@ -1,0 +1,215 @@
+/*
+ * spt_b200.h -- C ABI of the B200 (sm_100a) backend for the
+ * specific_particle_tracer hot path (AdamCBartnik/BEM).
+ *
+ * Plain C: fixed-width integers, doubles and raw pointers only.  Every data
+ * pointer is a DEVICE pointer on the current CUDA device unless a comment
+ * says otherwise; the caller allocates and owns all of them (the library
+ * never frees caller memory).  Every entry point returns SPT_OK (0) or an
+ * error code, and records a message readable with spt_last_error().  A
+ * call enqueues work on `stream` (a cudaStream_t passed as void*; NULL is
+ * the legacy default stream) and does not synchronise.
+ *
+ * Reference interfaces each entry point replaces (paths inside the
+ * reference project):
+ *   spt_trace      batched_rk45.integrate(accel_fn, pos0, vel0, t_birth, t_max,
+ *                  rtol, atol, kill_fn=...)            batched_rk45.py:55-323
+ *                  with accel_fn = geometry.make_accel_fn(...) geometry.py:265-301
+ *                  and kill_fn = geometry.make_kill_fn(...) geometry.py:304-322
+ *   spt_accel      the accel(pos, vel, active, group_idx) closure geometry.py:289-299
+ *   spt_bem_field  AxisymmetricBEMSolution.field(points)  bem/axisymmetric.py:474-487
+ *                  -> evaluate_axisymmetric_field         bem/axisymmetric.py:501-605
+ *   spt_ring_field ring_field(rho, z, a)                  bem/axisymmetric.py:235-265
+ *   spt_ellip_ke   ellip_ke_complement(p)                 bem/_elliptic.py:28-39
+ *   spt_bem_assemble  the collocation matrix of AxisymmetricBEMSolution.solve
+ *                  (adaptive _segment_potential)          bem/axisymmetric.py:275-302, 411-443
+ */
+#ifndef SPT_B200_H
+#define SPT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPT_ABI_VERSION 1
+
+/* return codes */
+#define SPT_OK 0
+#define SPT_ERR_ARG 1        /* invalid argument (shape, size, null pointer, alignment) */
+#define SPT_ERR_CUDA 2       /* a CUDA runtime call failed */
+#define SPT_ERR_CAPACITY 3   /* a size exceeds a documented maximum */
+
+/* geometry kinds (Geometry subclasses of geometry.py / bem/geometry.py) */
+#define SPT_GEOM_FLAT 0      /* geometry.FlatCathode                       geometry.py:97-163 */
+#define SPT_GEOM_TIP 1       /* geometry.HemisphericalTip                  geometry.py:166-256 */
+#define SPT_GEOM_TIP_BEM 2   /* bem.geometry.HemisphericalTipBEMGeometry, z0=None  bem/geometry.py:58-507 */
+#define SPT_GEOM_WELL_BEM 3  /* bem.geometry.CylindricalWellBEMGeometry, z0=None   bem/geometry.py:510-885 */
+#define SPT_GEOM_POST_BEM 4  /* hemisphere on a cylindrical post: capsule BEM field, 3-image force in the apex frame */
+
+/* arithmetic forms */
+#define SPT_FORM_FP64 0      /* plain: float64 throughout */
+#define SPT_FORM_MIXED 1     /* pair and BEM panel sums in float32 with Kahan compensation */
+
+/* per-group status (SptState.status) */
+#define SPT_GROUP_NEW 0      /* not started: t, h are initialised on first touch */
+#define SPT_GROUP_RUNNING 1
+#define SPT_GROUP_DONE 2     /* t >= t_max (1 - 1e-14)  (batched_rk45.py:317) */
+#define SPT_GROUP_NONFINITE 3/* the error norm became NaN: group stopped */
+#define SPT_GROUP_TIMEOUT 4  /* a bounded device wait gave up (TMA tile never arrived) */
+
+/* device counters (SptTraceParams.counters, accumulated, uint64) */
+#define SPT_CNT_ATTEMPTS 0           /* group-step attempts */
+#define SPT_CNT_ACCEPTED 1           /* accepted group-steps */
+#define SPT_CNT_PARTICLE_STEPS 2     /* sum over accepted group-steps of the group size */
+#define SPT_CNT_STAGE_EVALS 3        /* particle-stage evaluations (7 per particle-attempt) */
+#define SPT_CNT_PAIR_EVALS 4         /* pair interactions summed (all image sets included) */
+#define SPT_CNT_RING_FAR 5           /* far-quadrature ring-kernel evaluations */
+#define SPT_CNT_RING_NEAR 6          /* near (sinh-quadrature) ring-kernel evaluations */
+#define SPT_CNT_NEAR_PAIRS 7         /* (point, segment) pairs handled by the near quadrature */
+#define SPT_N_COUNTERS 8
+
+/* Geometry parameters.  Fields a kind does not use are ignored. */
+typedef struct {
+    int32_t kind;            /* SPT_GEOM_* */
+    int32_t has_image;       /* image-charge force on (z0 given) */
+    int32_t has_kill_below;  /* kill at z <= kill_z_below */
+    int32_t has_z_max;       /* kill at z >= z_max (geometry.make_kill_fn) */
+    double E_gun;            /* asymptotic field Ez [V/m] */
+    double R;                /* tip / post / well radius [m] */
+    double H;                /* well depth [m] */
+    double L;                /* post height = apex sphere centre z [m] */
+    double z0;               /* image-plane recession [m] */
+    double kill_z_below;
+    double z_max;
+    double z_handoff;        /* BEM below z_handoff/2, flat fallback above z_handoff */
+    double bottom_fillet;    /* well corner rounding radii [m] (0 = sharp) */
+    double rim_fillet;
+} SptGeometry;
+
+/* Number of per-segment fields in SptBem.seg (structure of arrays, each
+ * n_seg doubles, row stride seg_stride):
+ *   0 p0_rho  1 p0_z  2 tan_rho  3 tan_z   (tan = p1 - p0)
+ *   4 length  5 unit_rho  6 unit_z  7 normal_rho  8 normal_z
+ *   9 sigma0 (density at p0)  10 sigma1 (density at p1)              */
+#define SPT_SEG_FIELDS 11
+
+/* Precomputed BEM solution tables (bem/axisymmetric.py:305-338, 490-498).
+ * `node` holds 3 rows of node_stride doubles: rho_q, z_q, w_q = area_q*sigma_q
+ * for the n_seg*nodes_per_seg Gauss-4 far-quadrature nodes, segment-major.
+ * node_stride must be even (16-byte rows); the device pointers must be
+ * 16-byte aligned (tiles are copied with the TMA bulk engine). */
+typedef struct {
+    int32_t n_seg;
+    int32_t nodes_per_seg;   /* 4 * n_subdiv, at most 1024 */
+    int64_t seg_stride;
+    int64_t node_stride;
+    const double* seg;
+    const double* node;
+    double gauss8_x[8];      /* Gauss-Legendre 8-point nodes/weights on [-1, 1] */
+    double gauss8_w[8];
+} SptBem;
+
+/* Particle and per-group integrator state, in/out. Groups are contiguous
+ * particle ranges [group_offset[g], group_offset[g+1]). */
+typedef struct {
+    int32_t n_groups;
+    int32_t max_group_size;  /* max over g of group size */
+    int64_t n_particles;
+    const int64_t* group_offset;   /* [n_groups+1] */
+    const int32_t* group_order;    /* [n_groups] processing order (e.g. largest first) or NULL */
+    double* x; double* y; double* z;
+    double* vx; double* vy; double* vz;
+    const double* t_birth;
+    double* t_death;               /* +inf while alive; set to the step end time when killed */
+    const double* charge;          /* signed charge [C] */
+    const double* mass;            /* per-particle mass [kg] */
+    double* t;                     /* [n_groups] group clock */
+    double* h;                     /* [n_groups] next step size */
+    int32_t* status;               /* [n_groups] SPT_GROUP_* */
+    int64_t* n_accepted;           /* [n_groups] */
+    int64_t* n_rejected;           /* [n_groups] */
+} SptState;
+
+typedef struct {
+    double t_max, rtol, atol;
+    double plummer_radius;
+    double charge_to_mass;         /* species q/m for the external-field term */
+    double coulomb_constant;       /* 1/(4 pi eps0) [N m^2 C^-2] (constants.py:14) */
+    double safety, min_factor, max_factor, initial_step_fraction;
+    int64_t max_attempts;          /* attempts per group in this call */
+    int32_t form;                  /* SPT_FORM_* */
+    int32_t log_capacity;          /* entries per group in log_h/log_err (0: no log) */
+    double* log_h;                 /* [n_groups][log_capacity] step used by attempt k */
+    double* log_err;               /* [n_groups][log_capacity] its error norm */
+    unsigned long long* counters;  /* [SPT_N_COUNTERS] or NULL */
+} SptTraceParams;
+
+/* Scratch bytes spt_trace needs for this state/geometry (work-queue
+ * counter, and per-CTA group buffers when a group does not fit shared
+ * memory). Host-only; no device work. */
+int spt_trace_workspace_bytes(const SptState* state, const SptTraceParams* params,
+                              const SptGeometry* geom, const SptBem* bem, int64_t* bytes);
+
+/* Advance every group with status NEW or RUNNING by at most
+ * params->max_attempts Dormand-Prince 5(4) attempts (one persistent kernel,
+ * one CTA per group at a time, groups taken from a device work queue).
+ * `bem` may be NULL for SPT_GEOM_FLAT / SPT_GEOM_TIP. `workspace` is a
+ * device buffer of at least spt_trace_workspace_bytes() bytes, 256-byte
+ * aligned; the call clears what it needs. */
+int spt_trace(const SptState* state, const SptTraceParams* params, const SptGeometry* geom,
+              const SptBem* bem, void* workspace, int64_t workspace_bytes, void* stream);
+
+/* One stage evaluation (the accel closure): acc = (q/m)_s E(pos)
+ * + F_coulomb/m + F_image/m on active particles, 0 elsewhere.
+ * pos_*, acc_* are [n_particles]; active is uint8 [n_particles]. */
+typedef struct {
+    int32_t n_groups;
+    int32_t max_group_size;
+    int64_t n_particles;
+    const int64_t* group_offset;
+    const double* x; const double* y; const double* z;
+    const uint8_t* active;
+    const double* charge;
+    const double* mass;
+    double charge_to_mass;
+    double coulomb_constant;
+    double plummer_radius;
+    int32_t form;
+    double* ax; double* ay; double* az;
+} SptAccelArgs;
+int spt_accel(const SptAccelArgs* args, const SptGeometry* geom, const SptBem* bem, void* stream);
+
+/* Perturbation field E = -grad S[sigma] of the BEM solution at n points
+ * (x, y, z) -> (ex, ey, ez), all [n] device arrays. */
+int spt_bem_field(const double* x, const double* y, const double* z, int64_t n, const SptBem* bem,
+                  int32_t form, double* ex, double* ey, double* ez, void* stream);
+
+/* Unit-charge ring field (E_rho, E_z) at (rho, z) for ring radius a; [n]. */
+int spt_ring_field(const double* rho, const double* z, const double* a, int64_t n, int32_t form,
+                   double* er, double* ez, void* stream);
+
+/* K(1-p), E(1-p) for p in (0, 1]; [n]. */
+int spt_ellip_ke(const double* p, int64_t n, int32_t form, double* K, double* E, void* stream);
+
+/* Collocation matrix of the P1 single-layer BEM on a generating profile
+ * (bem/axisymmetric.py:411-443): A [n_nodes x n_nodes], row-major, A[i][j] =
+ * potential at node i of the unit hat density of node j, by adaptive
+ * bisection (refine while segment length > refine_ratio * distance, up to
+ * max_depth levels) with the 4-point Gauss rule (gauss4_x/w, device arrays of
+ * 4) on each leaf.  profile_rho/z are [n_nodes] device arrays. */
+int spt_bem_assemble(const double* profile_rho, const double* profile_z, int32_t n_nodes, double refine_ratio,
+                     int32_t max_depth, const double* gauss4_x, const double* gauss4_w, double* A, void* stream);
+
+/* Last error message of the calling thread (NUL-terminated, truncated to
+ * len). Returns the length of the full message. */
+int spt_last_error(char* buf, int32_t len);
+
+/* SPT_ABI_VERSION. */
+int spt_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPT_B200_H */

@@ -317,7 +317,17 @@ def gen_tracker():
     _save("tracker_flat", **out)
 
 
-GENERATORS = dict(ellip=gen_ellip, ring=gen_ring, accel=gen_accel, bem_sphere=gen_bem_sphere,
+def gen_sigma_c1():
+    """Reference solve of the 2000-panel hemisphere-on-post capsule
+    (R = 50 nm, L = 5 um, 100 cap + 900 wall segments per half), Ez = -1e6."""
+    from specific_particle_tracer.bem.axisymmetric import AxisymmetricBEMSolution
+    from bem_b200.mesh import capsule_profile
+    prof = capsule_profile(50e-9, 5e-6, 100, 900)
+    sol = AxisymmetricBEMSolution.solve(prof, dirichlet_fn=lambda rho, z: -1e6 * z)
+    _save("sigma_c1", profile=prof, sigma=sol.sigma, E_gun=-1e6)
+
+
+GENERATORS = dict(sigma_c1=gen_sigma_c1, ellip=gen_ellip, ring=gen_ring, accel=gen_accel, bem_sphere=gen_bem_sphere,
                   bem_well=gen_bem_well, bem_post=gen_bem_post, trace_flat=gen_trace_flat,
                   trace_tip=gen_trace_tip, trace_tip_bem=gen_trace_bem, trace_post=gen_trace_post,
                   trace_well=gen_trace_well, tracker=gen_tracker,
@@ -330,7 +340,7 @@ def main():
     ap.add_argument("names", nargs="*")
     a = ap.parse_args()
     _setup(a.ref)
-    for name in a.names or [k for k in GENERATORS if k != "trace_flat_c0"]:
+    for name in a.names or [k for k in GENERATORS if k not in ("trace_flat_c0", "sigma_c1")]:
         t0 = time.time()
         GENERATORS[name]()
         print(f"{name}: {time.time() - t0:.1f}s")
