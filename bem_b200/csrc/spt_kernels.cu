@@ -39,7 +39,8 @@ namespace spt {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRound = 8;           // points per far-sum round
-constexpr int kTileNodes = 1024;    // nodes per TMA tile
+constexpr int kTileNodes = 2048;    // nodes per TMA tile row (largest; halved while shared memory is short)
+constexpr size_t kMaxSmem = 226 * 1024;  // dynamic part; the static __shared__ scalars take the rest of 227 KB
 constexpr int kSmallGroup = 256;    // groups above this keep slopes in global memory
 
 // Dormand-Prince 5(4) tableau (batched_rk45.py:30-50).
@@ -81,7 +82,7 @@ __device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t
 // ran out (the caller flags the group instead of spinning forever).
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
     uint32_t done = 0;
-    for (int it = 0; it < (1 << 24); ++it) {
+    for (int it = 0; it < (1 << 22); ++it) {
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
             : "=r"(done)
@@ -186,7 +187,8 @@ struct Layout {
     int fld;                  // 3E field
     int img;                  // 4E sphere images
     int bpt;                  // 8E per BEM list entry: x y z rho_e z_e near_r near_z (+1 pad)
-    int tiles;                // 2 * 3 * kTileNodes
+    int tiles;                // 2 * 3 * tile_cap
+    int tile_cap;             // nodes per TMA tile row
     int red;                  // kWarps * 2 * kRound
     int ints;                 // int region start (in doubles)
     int total_doubles;
@@ -218,15 +220,21 @@ __host__ __device__ inline Layout make_layout(int E, bool want_tiles) {
     L.img = o; o += 4 * E;
     L.bpt = o; o += 8 * E;
     o = (o + 1) & ~1;  // 16-byte alignment for the TMA tiles
-    L.tiles = o; o += want_tiles ? 2 * 3 * kTileNodes : 0;
-    L.red = o; o += kWarps * 2 * kRound;
-    L.ints = o;
+    const int base = o;
+    const int n_ints = 2 * E + kRound * 256 / 4 + 4;  // live, list, near flags (bytes) packed in ints
+    for (int cap = kTileNodes; cap >= 256; cap >>= 1) {
+        o = base;
+        L.tile_cap = cap;
+        L.tiles = o; o += want_tiles ? 2 * 3 * cap : 0;
+        L.red = o; o += kWarps * 2 * kRound;
+        L.ints = o;
+        L.total_doubles = o + (n_ints + 1) / 2;
+        L.bytes = (size_t)L.total_doubles * 8 + 64;  // + mbarriers
+        if (L.bytes <= kMaxSmem) break;
+    }
     L.live_off = 0;
     L.list_off = E;
     L.flags_off = 2 * E;
-    const int n_ints = 2 * E + kRound * 256 / 4 + 4;  // live, list, near flags (bytes) packed in ints
-    L.total_doubles = o + (n_ints + 1) / 2;
-    L.bytes = (size_t)L.total_doubles * 8 + 64;  // + mbarriers
     return L;
 }
 
@@ -248,6 +256,7 @@ struct Ctx {
     int* list;
     unsigned char* nflag;
     uint64_t* bars;
+    uint32_t phase[2];          // parity of the next phase to wait for on bars[0], bars[1] (identical in every thread)
     unsigned long long cnt[8];  // per-thread counter partials (thread 0 flushes)
 };
 
@@ -295,15 +304,17 @@ struct Seg {
 
 __device__ __forceinline__ double segf(const SptBem& b, int f, int s) { return __ldg(b.seg + (size_t)f * b.seg_stride + s); }
 
-// closest-point distance^2 of (rq, zq) to segment s (bem/axisymmetric.py:117-133)
+// closest-point distance^2 of (rq, zq) to segment s (bem/axisymmetric.py:117-133,
+// 374-381), with no FMA contraction: the on-surface offset below is a
+// threshold test on this value, so it is rounded like the reference's.
 __device__ __forceinline__ double seg_dist2(const SptBem& b, int s, double rq, double zq) {
     const double p0x = segf(b, 0, s), p0y = segf(b, 1, s), ax = segf(b, 2, s), ay = segf(b, 3, s);
-    const double ab = ax * ax + ay * ay;
-    double t = ((rq - p0x) * ax + (zq - p0y) * ay) / ab;
+    const double ab = __dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay));
+    double t = __ddiv_rn(__dadd_rn(__dmul_rn(__dadd_rn(rq, -p0x), ax), __dmul_rn(__dadd_rn(zq, -p0y), ay)), ab);
     t = fmin(fmax(t, 0.0), 1.0);
-    const double cr = p0x + t * ax, cz = p0y + t * ay;
-    const double dr = rq - cr, dz = zq - cz;
-    return dr * dr + dz * dz;
+    const double cr = __dadd_rn(p0x, __dmul_rn(t, ax)), cz = __dadd_rn(p0y, __dmul_rn(t, ay));
+    const double dr = __dadd_rn(rq, -cr), dz = __dadd_rn(zq, -cz);
+    return __dadd_rn(__dmul_rn(dr, dr), __dmul_rn(dz, dz));
 }
 
 // near test of bem/axisymmetric.py:566-570 -> (near, projection, distance)
@@ -315,6 +326,117 @@ __device__ __forceinline__ bool seg_near(const SptBem& b, int s, double re, doub
     const double ar = dr - proj * ur, az = dz - proj * uz;
     dist = sqrt(ar * ar + az * az);
     return dist < L;
+}
+
+
+// One far-sum round for points r0..r0+np_-1 of the list (np_ <= NP): the
+// node table streams through shared memory in TMA tiles (double buffered);
+// each thread takes NQ nodes at a time, strided by the CTA width, against
+// all NP points (NP * NQ independent ring evaluations per iteration).
+template <int NP, int NQ>
+__device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_tile, bool& ok,
+                          unsigned long long& far_evals) {
+    const SptBem& b = c.bem;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nseg = b.n_seg, nps = b.nodes_per_seg;
+    const int tile_cap = c.L.tile_cap;
+    double* P = c.bpt;
+    double* tile[2] = {c.tiles, c.tiles + 3 * tile_cap};
+    uint64_t* bars = c.bars;
+    double pr[NP], pinv[NP], pz[NP], ar[NP], az[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        const int k = r0 + (p < np_ ? p : 0);
+        pr[p] = P[8 * k + 3];
+        pinv[p] = pr[p] > 0.0 ? 1.0 / pr[p] : 0.0;
+        pz[p] = P[8 * k + 4];
+        ar[p] = 0.0;
+        az[p] = 0.0;
+    }
+    auto issue = [&](int t, int buf) {
+        const int s_first = t * segs_per_tile;
+        const int nn = min(segs_per_tile, nseg - s_first) * nps;
+        const uint32_t bytes = (uint32_t)nn * 8u;
+        mbar_expect_tx(&bars[buf], 3u * bytes);
+        for (int row = 0; row < 3; ++row)
+            tma_load_1d(tile[buf] + row * tile_cap, b.node + (size_t)row * b.node_stride + (size_t)s_first * nps, bytes,
+                        &bars[buf]);
+    };
+    if (tid == 0) {
+        issue(0, 0);
+        if (n_tiles > 1) issue(1, 1);
+    }
+    for (int t = 0; t < n_tiles; ++t) {
+        const int buf = t & 1;
+        const int s_first = t * segs_per_tile;
+        const int ns = min(segs_per_tile, nseg - s_first);
+        for (int idx = tid; idx < np_ * ns; idx += kThreads) {
+            const int p = idx / ns, sl = idx - p * ns;
+            double proj, dist;
+            c.nflag[p * 256 + sl] = seg_near(b, s_first + sl, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4], proj, dist);
+        }
+        if (!mbar_wait(&bars[buf], c.phase[buf])) ok = false;
+        c.phase[buf] ^= 1u;
+        __syncthreads();
+        if (ok) {
+            const double* tr = tile[buf];
+            const double* tz = tr + tile_cap;
+            const double* tw = tz + tile_cap;
+            const int nn = ns * nps;
+            for (int q0 = tid; q0 < nn; q0 += kThreads * NQ) {
+                double rq[NQ], zq[NQ], wq[NQ];
+                int sl[NQ];
+                bool in[NQ];
+#pragma unroll
+                for (int j = 0; j < NQ; ++j) {
+                    const int q = q0 + j * kThreads;
+                    in[j] = q < nn;
+                    const int qq = in[j] ? q : 0;
+                    rq[j] = tr[qq];
+                    zq[j] = tz[qq];
+                    wq[j] = tw[qq];
+                    sl[j] = qq / nps;
+                }
+#pragma unroll
+                for (int p = 0; p < NP; ++p) {
+#pragma unroll
+                    for (int j = 0; j < NQ; ++j) {
+                        if (p < np_ && in[j] && !c.nflag[p * 256 + sl[j]]) {
+                            double er, ez;
+                            ring_field_far(pr[p], pinv[p], pz[p] - zq[j], rq[j], er, ez);
+                            ar[p] = fma(wq[j], er, ar[p]);
+                            az[p] = fma(wq[j], ez, az[p]);
+                            ++far_evals;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && t + 2 < n_tiles) issue(t + 2, buf);
+    }
+    // fixed-order block reduction of the round's accumulators
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        const double vr = warp_sum(ar[p]);
+        const double vz = warp_sum(az[p]);
+        if (lane == 0) {
+            c.red[warp * 2 * kRound + p] = vr;
+            c.red[warp * 2 * kRound + kRound + p] = vz;
+        }
+    }
+    __syncthreads();
+    if (tid < np_) {
+        double sr = 0.0, sz = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+            sr += c.red[w * 2 * kRound + tid];
+            sz += c.red[w * 2 * kRound + kRound + tid];
+        }
+        const int k = r0 + tid;
+        P[8 * k + 5] = sr + P[8 * k + 7];
+        P[8 * k + 6] = sz + c.fld[3 * k + 2];
+    }
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------------------
@@ -349,11 +471,12 @@ __device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
         if (lane == 0) {
             if (bs >= nseg) bs = 0;  // every distance was NaN: the reference keeps index 0
             const double Ls = segf(b, 4, bs);
-            const double off = (best < (1e-9 * Ls) * (1e-9 * Ls)) ? 1e-4 * Ls : 0.0;
-            double re = rho + off * segf(b, 7, bs);
+            const double thr = __dmul_rn(1e-9, Ls);
+            const double off = (best < __dmul_rn(thr, thr)) ? __dmul_rn(1e-4, Ls) : 0.0;
+            double re = __dadd_rn(rho, __dmul_rn(off, segf(b, 7, bs)));
             if (rho == 0.0) re = 0.0;
             P[8 * k + 3] = re;
-            P[8 * k + 4] = z + off * segf(b, 8, bs);
+            P[8 * k + 4] = __dadd_rn(z, __dmul_rn(off, segf(b, 8, bs)));
         }
     }
     __syncthreads();
@@ -406,101 +529,26 @@ __device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
     if (lane == 0) { c.cnt[SPT_CNT_NEAR_PAIRS] += n_near; c.cnt[SPT_CNT_RING_NEAR] += n_ring_near; }
     __syncthreads();
 
-    // C: far sum, rounds of kRound points over TMA-staged node tiles
-    const int segs_per_tile = kTileNodes / nps;
-    const int tile_nodes = segs_per_tile * nps;
+    // C: far sum, rounds of up to kRound points over TMA-staged node tiles;
+    // the round's point count selects how many nodes each thread keeps in
+    // flight so that every thread has 8 independent ring evaluations.
+    const int tile_cap = c.L.tile_cap;
+    const int segs_per_tile = min(tile_cap / nps, 256);
     const int n_tiles = (nseg + segs_per_tile - 1) / segs_per_tile;
-    double* tile[2] = {c.tiles, c.tiles + 3 * kTileNodes};
-    uint64_t* bars = c.bars;
     unsigned long long far_evals = 0;
+    bool ok = true;
     for (int r0 = 0; r0 < n; r0 += kRound) {
         const int np_ = min(kRound, n - r0);
-        double pr[kRound], pz[kRound], ar[kRound], az[kRound];
-#pragma unroll
-        for (int p = 0; p < kRound; ++p) {
-            const int k = r0 + (p < np_ ? p : 0);
-            pr[p] = P[8 * k + 3];
-            pz[p] = P[8 * k + 4];
-            ar[p] = 0.0;
-            az[p] = 0.0;
-        }
-        uint32_t phase[2] = {0, 0};
-        auto issue = [&](int t, int buf) {
-            const int s_first = t * segs_per_tile;
-            const int nn = min(segs_per_tile, nseg - s_first) * nps;
-            const uint32_t bytes = (uint32_t)nn * 8u;
-            mbar_expect_tx(&bars[buf], 3u * bytes);
-            for (int row = 0; row < 3; ++row)
-                tma_load_1d(tile[buf] + row * kTileNodes, b.node + (size_t)row * b.node_stride + (size_t)s_first * nps,
-                            bytes, &bars[buf]);
-        };
-        if (tid == 0) {
-            issue(0, 0);
-            if (n_tiles > 1) issue(1, 1);
-        }
-        bool ok = true;
-        for (int t = 0; t < n_tiles; ++t) {
-            const int buf = t & 1;
-            const int s_first = t * segs_per_tile;
-            const int ns = min(segs_per_tile, nseg - s_first);
-            // near flags for (point, segment) of this tile
-            for (int idx = tid; idx < np_ * ns; idx += kThreads) {
-                const int p = idx / ns, sl = idx - p * ns;
-                double proj, dist;
-                c.nflag[p * 256 + sl] = seg_near(b, s_first + sl, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4], proj, dist);
-            }
-            if (!mbar_wait(&bars[buf], phase[buf])) ok = false;
-            phase[buf] ^= 1u;
-            __syncthreads();
-            if (ok) {
-                const double* tr = tile[buf];
-                const double* tz = tr + kTileNodes;
-                const double* tw = tz + kTileNodes;
-                const int nn = ns * nps;
-                for (int qn = tid; qn < nn; qn += kThreads) {
-                    const int sl = qn / nps;
-                    const double rq = tr[qn], zq = tz[qn], wq = tw[qn];
-#pragma unroll
-                    for (int p = 0; p < kRound; ++p) {
-                        if (p < np_ && !c.nflag[p * 256 + sl]) {
-                            double er, ez;
-                            ring_field(pr[p], pz[p] - zq, rq, er, ez);
-                            ar[p] = fma(wq, er, ar[p]);
-                            az[p] = fma(wq, ez, az[p]);
-                            ++far_evals;
-                        }
-                    }
-                }
-            }
-            __syncthreads();
-            if (tid == 0 && t + 2 < n_tiles) issue(t + 2, buf);
-        }
-        if (!ok && tid == 0) *status_flag = SPT_GROUP_TIMEOUT;
-        // fixed-order block reduction of the round's accumulators
-#pragma unroll
-        for (int p = 0; p < kRound; ++p) {
-            const double vr = warp_sum(ar[p]);
-            const double vz = warp_sum(az[p]);
-            if (lane == 0) {
-                c.red[warp * 2 * kRound + p] = vr;
-                c.red[warp * 2 * kRound + kRound + p] = vz;
-            }
-        }
-        __syncthreads();
-        if (tid < np_) {
-            double sr = 0.0, sz = 0.0;
-            for (int w = 0; w < kWarps; ++w) {
-                sr += c.red[w * 2 * kRound + tid];
-                sz += c.red[w * 2 * kRound + kRound + tid];
-            }
-            const int k = r0 + tid;
-            const double e_rho = sr + P[8 * k + 7];
-            const double e_z = sz + c.fld[3 * k + 2];
-            P[8 * k + 5] = e_rho;
-            P[8 * k + 6] = e_z;
-        }
-        __syncthreads();
+        if (np_ == 1)
+            far_round<1, 8>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+        else if (np_ == 2)
+            far_round<2, 4>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+        else if (np_ <= 4)
+            far_round<4, 2>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+        else
+            far_round<8, 1>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
     }
+    if (!ok && tid == 0) *status_flag = SPT_GROUP_TIMEOUT;
     c.cnt[SPT_CNT_RING_FAR] += far_evals;
     // D: rotate E_rho into (x, y)
     for (int k = tid; k < n; k += kThreads) {
@@ -717,6 +765,8 @@ __device__ inline void flush_counters(Ctx& c, unsigned long long* counters) {
 }
 
 __device__ inline void init_barriers(Ctx& c) {
+    c.phase[0] = 0u;
+    c.phase[1] = 0u;
     if (threadIdx.x == 0) {
         mbar_init(&c.bars[0], 1);
         mbar_init(&c.bars[1], 1);
@@ -813,8 +863,10 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
                 gs.next_cp = gs.exhausted ? prm.t_max : c.cps[lo];
                 const double target = fmin(gs.next_cp, prm.t_max);
                 gs.hr = fmin(gs.h, target - gs.t);
+                if (!(gs.hr > 0.0) || !isfinite(gs.hr)) gs.status = SPT_GROUP_NONFINITE;
             }
             __syncthreads();
+            if (gs.status != SPT_GROUP_RUNNING) break;
             const double t = gs.t, hr = gs.hr;
             for (int i = tid; i < E; i += kThreads) c.live[i] = (t >= c.tb[i]) && (t < c.td[i]);
             __syncthreads();
@@ -943,6 +995,9 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
         }
         flush_counters(c, prm.counters);
         __syncthreads();
+        // A timed-out barrier wait leaves this CTA's barrier phases unknown:
+        // stop taking groups (the remaining ones stay NEW/RUNNING for the host).
+        if (s_flag == SPT_GROUP_TIMEOUT) break;
     }
 }
 
@@ -1127,8 +1182,8 @@ int cuda_check(cudaError_t e, const char* what) {
 
 int check_bem(const SptBem* b) {
     if (!b || !b->seg || !b->node) return fail(SPT_ERR_ARG, "BEM tables required for this geometry");
-    if (b->n_seg <= 0 || b->nodes_per_seg <= 0 || b->nodes_per_seg % 4 || b->nodes_per_seg > spt::kTileNodes)
-        return fail(SPT_ERR_ARG, "nodes_per_seg must be a positive multiple of 4, at most %d", spt::kTileNodes);
+    if (b->n_seg <= 0 || b->nodes_per_seg <= 0 || b->nodes_per_seg % 4 || b->nodes_per_seg > 256)
+        return fail(SPT_ERR_ARG, "nodes_per_seg must be a positive multiple of 4, at most 256");
     if ((reinterpret_cast<uintptr_t>(b->node) & 15) || (b->node_stride & 1))
         return fail(SPT_ERR_ARG, "node table must be 16-byte aligned with an even row stride");
     if (b->node_stride < (int64_t)b->n_seg * b->nodes_per_seg || b->seg_stride < b->n_seg)

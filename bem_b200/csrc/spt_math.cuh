@@ -94,6 +94,58 @@ __device__ __forceinline__ void ring_field(double rho, double z, double a, doubl
     ez = z * E / (2.0 * kPi * kPi * sD * d2);
 }
 
+
+// Same K(1-p), E(1-p) with a fixed six-step AGM (no data-dependent exit) so
+// several evaluations can be interleaved by the compiler.  For p >= 1e-3 the
+// sixth half-difference c_6 is below 1e-14, so a_6 has converged to the AGM
+// (its error is c_7 ~ 1e-28) and the neglected E-sum terms are below 1e-26.
+__device__ __forceinline__ void ellip_ke_fixed(double p, double& K, double& E) {
+    if (p < 1e-3) {
+        const double L = -0.5 * log(p);
+        K = fma(L, horner10(kSerK, p), horner10(kSerKd, p));
+        E = fma(0.5 * p, fma(L, horner10(kSerE, p), horner10(kSerEd, p)), 1.0);
+        return;
+    }
+    double a = 1.0, b = sqrt(p);
+    double S = 0.5 * (1.0 - p), w = 0.5;
+#pragma unroll
+    for (int it = 0; it < 6; ++it) {
+        const double c = 0.5 * (a - b);
+        const double an = 0.5 * (a + b);
+        b = sqrt(a * b);
+        a = an;
+        w += w;
+        S = fma(w * c, c, S);
+    }
+    K = (0.5 * kPi) / a;
+    E = K * (1.0 - S);
+}
+
+// Ring field for the far-quadrature sum: the formula of ring_field with one
+// reciprocal of D*d2 in place of the divisions by D and d2, and 1/rho
+// supplied by the caller (constant over a point's whole node loop).
+__device__ __forceinline__ void ring_field_far(double rho, double inv_rho, double z, double a, double& er,
+                                               double& ez) {
+    const double z2 = z * z, a2 = a * a, rho2 = rho * rho;
+    const double D = (rho + a) * (rho + a) + z2;
+    const double d2 = (rho - a) * (rho - a) + z2;
+    if (rho2 < 1e-10 * (a2 + z2)) {
+        const double ax2 = a2 + z2;
+        const double s = sqrt(ax2);
+        const double ax15 = ax2 * s, ax25 = ax2 * ax15, ax35 = ax2 * ax25;
+        er = rho * (2.0 * z2 - a2) / (8.0 * kPi * ax25);
+        ez = z / (4.0 * kPi * ax15) + 3.0 * rho2 * z * (3.0 * a2 - 2.0 * z2) / (16.0 * kPi * ax35);
+        return;
+    }
+    const double inv = 1.0 / (D * d2);
+    const double invD = d2 * inv, inv_d2 = D * inv;
+    double K, E;
+    ellip_ke_fixed(d2 * invD, K, E);
+    const double rsD = sqrt(invD);
+    er = (K - (a2 - rho2 + z2) * E * inv_d2) * (rsD * inv_rho * (1.0 / (4.0 * kPi * kPi)));
+    ez = z * E * rsD * inv_d2 * (1.0 / (2.0 * kPi * kPi));
+}
+
 // ---------------------------------------------------------------------------
 // float32 variants (SPT_FORM_MIXED).  Same methods; the series branch is
 // used below p < 1e-2 with four terms (truncation < 1e-9), the AGM above.

@@ -16,7 +16,7 @@ import numpy as np
 from . import _lib
 from .constants import COULOMB_CONSTANT
 
-DEFAULT_ATTEMPT_CHUNK = 1 << 30
+DEFAULT_ATTEMPT_CHUNK = 4096  # attempts per group per launch; the host loops until every group is done
 
 
 def _torch():

@@ -65,8 +65,8 @@ class BemTables:
     def __init__(self, profile, sigma, n_subdiv=8, device="cuda"):
         import torch
 
-        if not (1 <= n_subdiv <= 256):
-            raise ValueError("n_subdiv must be in [1, 256]")
+        if not (1 <= n_subdiv <= 64):
+            raise ValueError("n_subdiv must be in [1, 64]")
         self.profile = np.asarray(profile, dtype=np.float64)
         self.sigma = np.asarray(sigma, dtype=np.float64)
         self.n_subdiv = int(n_subdiv)

@@ -144,9 +144,8 @@ def prepare_cpu_blob(name, wl):
     spec = wl["geometry"].spec()
     d = {k: v for k, v in wl["data"].items()}
     blob = dict(spec=spec, data=d, rtol=wl["rtol"], atol=wl["atol"], t_max=wl["t_max"], z_max=wl["z_max"])
-    path = os.path.join(REPO, "gpurun_out" if os.path.isdir(os.path.join(REPO, "gpurun_out")) else "_work",
-                        f"cpu_blob_{name}.npz")
-    os.makedirs(os.path.dirname(path), exist_ok=True)
+    import tempfile
+    path = os.path.join(tempfile.gettempdir(), f"spt_bench_cpu_{name}_{os.getpid()}.npz")
     np.savez(path, wl=np.array(blob, dtype=object))
     os.environ["SPT_BENCH_CPU_BLOB"] = path
     return path
@@ -346,13 +345,13 @@ def load_traffic(workload, form):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2", "c3", "c4"])
-    ap.add_argument("--attempts", type=int, default=4, help="RK45 attempts per group per step")
+    ap.add_argument("--attempts", type=int, default=16, help="RK45 attempts per group per step")
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--cpu-attempts", type=int, default=6)
+    ap.add_argument("--cpu-attempts", type=int, default=16)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()

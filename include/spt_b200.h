@@ -102,7 +102,7 @@ typedef struct {
  * 16-byte aligned (tiles are copied with the TMA bulk engine). */
 typedef struct {
     int32_t n_seg;
-    int32_t nodes_per_seg;   /* 4 * n_subdiv, at most 1024 */
+    int32_t nodes_per_seg;   /* 4 * n_subdiv, at most 256 */
     int64_t seg_stride;
     int64_t node_stride;
     const double* seg;
