@@ -74,6 +74,8 @@ SIGNATURES = {
     "spt_ring_field": (ctypes.c_int, [_p, _p, _p, _i64, _i32, _p, _p, _p]),
     "spt_ellip_ke": (ctypes.c_int, [_p, _i64, _i32, _p, _p, _p]),
     "spt_bem_assemble": (ctypes.c_int, [_p, _p, _i32, _d, _i32, _p, _p, _p, _p]),
+    "spt_trace_noalloc": (ctypes.c_int, [ctypes.POINTER(SptState), ctypes.POINTER(SptTraceParams),
+                                         ctypes.POINTER(SptGeometry), ctypes.POINTER(SptBem), _p]),
 }
 
 _LIB = None

@@ -1363,3 +1363,94 @@ int spt_bem_assemble(const double* profile_rho, const double* profile_z, int32_t
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// spt_trace_noalloc: spt_trace for callers that cannot allocate device memory.
+//
+// Its scratch (the work-queue counter and, for groups above 256 particles,
+// the per-CTA slope buffers) is this file-scope device array, so the call
+// needs no workspace and allocates nothing.  The array is part of the
+// library image: every GPU that loads the library holds its 4 MiB until the
+// process exits.  Host code cannot use `g_noalloc_scratch` as an address --
+// on the host that name is only a stand-in -- so its device address is
+// looked up once per device with cudaGetSymbolAddress, with that device
+// current, on the first call made on that device.
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(4) << 20;
+}
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+void* g_noalloc_ptr[64] = {nullptr};
+
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
+    if (rc) return rc;
+    if (dev < 0 || dev >= 64) return fail(SPT_ERR_CAPACITY, "device index %d above 63", dev);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        rc = cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(g_noalloc_scratch)");
+        if (rc) return rc;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return SPT_OK;
+}
+
+template <int KIND>
+int launch_trace_noalloc(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b,
+                         unsigned char* scratch, cudaStream_t stream) {
+    const spt::Layout L = spt::make_layout(s->max_group_size, true);
+    auto kern = spt::trace_kernel<KIND>;
+    int rc = set_smem(kern, L.bytes);
+    if (rc) return rc;
+    int per_sm = 0;
+    rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, spt::kThreads, L.bytes), "occupancy");
+    if (rc) return rc;
+    if (per_sm < 1) return fail(SPT_ERR_CAPACITY, "group size %d does not fit one CTA", s->max_group_size);
+    int grid = grid_for(s->n_groups, per_sm);
+    double* slots = nullptr;
+    if (L.big) {
+        // the persistent grid is capped by the number of slope slots the fixed scratch holds
+        const size_t slot_bytes = spt::big_slot_doubles(s->max_group_size) * 8;
+        const long long fit = (long long)((kNoAllocScratchBytes - 256) / slot_bytes);
+        if (fit < 1) return fail(SPT_ERR_CAPACITY, "spt_trace_noalloc: one group buffer exceeds the %zu-byte scratch",
+                                 kNoAllocScratchBytes);
+        if (grid > fit) grid = (int)fit;
+        slots = reinterpret_cast<double*>(scratch + 256);
+    }
+    // the counter must start at zero; the slot buffers are written before they are read
+    rc = cuda_check(cudaMemsetAsync(scratch, 0, sizeof(int), stream), "cudaMemsetAsync");
+    if (rc) return rc;
+    SptBem bem = b ? *b : SptBem{};
+    kern<<<grid, spt::kThreads, L.bytes, stream>>>(*s, *p, *g, bem, reinterpret_cast<int*>(scratch), slots);
+    return cuda_check(cudaGetLastError(), "trace_kernel launch");
+}
+}  // namespace
+
+extern "C" int spt_trace_noalloc(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b,
+                                 void* stream) {
+    if (!s || !p || !g) return fail(SPT_ERR_ARG, "null argument");
+    if (s->n_groups <= 0) return SPT_OK;
+    if (s->max_group_size <= 0 || s->max_group_size > 1024)
+        return fail(SPT_ERR_CAPACITY, "spt_trace_noalloc: max_group_size %d outside [1, 1024]", s->max_group_size);
+    if (p->form != SPT_FORM_FP64 && p->form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "unknown form %d", p->form);
+    if (is_bem(g->kind)) {
+        const int rc = check_bem(b);
+        if (rc) return rc;
+    }
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    unsigned char* sc = static_cast<unsigned char*>(scratch);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    switch (g->kind) {
+        case SPT_GEOM_FLAT: return launch_trace_noalloc<SPT_GEOM_FLAT>(s, p, g, b, sc, st);
+        case SPT_GEOM_TIP: return launch_trace_noalloc<SPT_GEOM_TIP>(s, p, g, b, sc, st);
+        case SPT_GEOM_TIP_BEM: return launch_trace_noalloc<SPT_GEOM_TIP_BEM>(s, p, g, b, sc, st);
+        case SPT_GEOM_WELL_BEM: return launch_trace_noalloc<SPT_GEOM_WELL_BEM>(s, p, g, b, sc, st);
+        case SPT_GEOM_POST_BEM: return launch_trace_noalloc<SPT_GEOM_POST_BEM>(s, p, g, b, sc, st);
+        default: return fail(SPT_ERR_ARG, "unknown geometry kind %d", g->kind);
+    }
+}

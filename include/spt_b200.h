@@ -202,6 +202,27 @@ int spt_ellip_ke(const double* p, int64_t n, int32_t form, double* K, double* E,
 int spt_bem_assemble(const double* profile_rho, const double* profile_z, int32_t n_nodes, double refine_ratio,
                      int32_t max_depth, const double* gauss4_x, const double* gauss4_w, double* A, void* stream);
 
+/* spt_trace for callers that cannot allocate device memory: a caller with no
+ * device allocator of its own (a cgo/JNI/ctypes binding without torch), or
+ * one running where a cudaMalloc would implicitly synchronise the device and
+ * stall other streams, or one whose device memory is fully reserved by
+ * another framework's pool.  Same state, parameters and results as
+ * spt_trace, but no workspace: the scratch is a fixed 4 MiB device array
+ * inside the library, held on every GPU that loads the library until the
+ * process exits.  No counterpart in the reference.
+ *   - max_group_size must be in [1, 1024] (SPT_ERR_CAPACITY otherwise); for
+ *     groups above 256 particles the scratch holds floor((4 MiB - 256) /
+ *     (432 * max_group_size)) per-CTA buffers, which caps the number of
+ *     CTAs that run at once (9 at 1024 particles).
+ *   - The first call on a device looks the array's address up
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture.
+ *   - Every call shares the one array: calls that overlap on the GPU (other
+ *     streams, other host threads) race on it; serialise them.  Each call
+ *     clears the work-queue counter it needs; nothing else carries over. */
+int spt_trace_noalloc(const SptState* state, const SptTraceParams* params, const SptGeometry* geom,
+                      const SptBem* bem, void* stream);
+
 /* Last error message of the calling thread (NUL-terminated, truncated to
  * len). Returns the length of the full message. */
 int spt_last_error(char* buf, int32_t len);
