@@ -49,7 +49,10 @@ class SptTraceParams(ctypes.Structure):
     _fields_ = [("t_max", _d), ("rtol", _d), ("atol", _d), ("plummer_radius", _d), ("charge_to_mass", _d),
                 ("coulomb_constant", _d), ("safety", _d), ("min_factor", _d), ("max_factor", _d),
                 ("initial_step_fraction", _d), ("max_attempts", _i64), ("form", _i32), ("log_capacity", _i32),
-                ("log_h", _p), ("log_err", _p), ("counters", _p)]
+                ("log_h", _p), ("log_err", _p), ("counters", _p),
+                ("n_screens", _i32), ("n_outputs", _i32), ("screens", _p), ("screen_rec", _p),
+                ("screen_capacity", _i64), ("screen_count", _p), ("output_times", _p), ("output_rec", _p),
+                ("output_flag", _p)]
 
 
 class SptAccelArgs(ctypes.Structure):

@@ -779,10 +779,98 @@ __device__ inline void init_barriers(Ctx& c) {
 // the persistent integrator
 
 struct GroupScalars {
-    double t, h, hr, next_cp, err, h_next;
-    int status, exhausted, accepted;
+    double t, h, hr, next_cp, err, h_next, next_out;
+    int status, exhausted, accepted, out_ptr, out_exh, fire_out;
     long long n_acc, n_rej;
 };
+
+// number of entries of the ascending array v[0..n) that are <= x
+__device__ __forceinline__ int count_le(const double* v, int n, double x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (v[mid] <= x) lo = mid + 1; else hi = mid;
+    }
+    return lo;
+}
+
+// Cubic Hermite pieces (screens.py:118-152), evaluated in the reference's order.
+__device__ __forceinline__ double hermite_z(double p0, double v0, double p1, double v1, double dt, double s) {
+    const double s2 = s * s, s3 = s2 * s;
+    const double h00 = 2 * s3 - 3 * s2 + 1, h10 = s3 - 2 * s2 + s, h01 = -2 * s3 + 3 * s2, h11 = s3 - s2;
+    return h00 * p0 + h10 * dt * v0 + h01 * p1 + h11 * dt * v1;
+}
+
+__device__ __forceinline__ double sgn(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
+
+// Screen crossings of one particle over one accepted step (screens.py:43-115,
+// 155-168): the Hermite z(s) is split at its extrema so each bracket is
+// monotone; a sign change over a bracket is located by 60 bisections and the
+// crossing state (Hermite position and derivative) is appended to the record
+// buffer.  Half-open (t_old, t_new]: a start exactly on the screen is not a crossing.
+__device__ void screen_crossings(const SptTraceParams& prm, const double* o, const double* n, double t_old,
+                                 double dt, long long particle) {
+    const double z0 = o[2], z1 = n[2];
+    bool moving = false;
+    for (int k = 0; k < 6; ++k) moving |= (o[k] != n[k]);
+    if (!moving || !(dt > 0.0)) return;
+    const double u0 = dt * o[5], u1 = dt * n[5];
+    double A = 3 * (2 * (z0 - z1) + u0 + u1);
+    double B = 2 * (3 * (z1 - z0) - 2 * u0 - u1);
+    double C = u0;
+    double sc = fmax(fmax(fabs(A), fabs(B)), fabs(C));
+    sc = sc > 0.0 ? sc : 1.0;
+    A /= sc; B /= sc; C /= sc;
+    const double disc = B * B - 4 * A * C;
+    const double q = -0.5 * (B + (B >= 0.0 ? 1.0 : -1.0) * sqrt(fmax(disc, 0.0)));
+    double r0 = q / (A != 0.0 ? A : 1.0);
+    const double r1 = C / (q != 0.0 ? q : 1.0);
+    const double lin = -C / (B != 0.0 ? B : 1.0);
+    if (A == 0.0) r0 = lin;
+    const bool v0 = (disc >= 0.0) && (A != 0.0 || B != 0.0) && (r0 > 0.0) && (r0 < 1.0);
+    const bool v1 = (disc >= 0.0) && (A != 0.0) && (q != 0.0) && (r1 > 0.0) && (r1 < 1.0);
+    double cut[4] = {0.0, v0 ? r0 : 1.0, v1 ? r1 : 1.0, 1.0};
+    if (cut[1] > cut[2]) { const double tmp = cut[1]; cut[1] = cut[2]; cut[2] = tmp; }
+    for (int sidx = 0; sidx < prm.n_screens; ++sidx) {
+        const double zs = prm.screens[sidx];
+        for (int iv = 0; iv < 3; ++iv) {
+            const double left = cut[iv], right = cut[iv + 1];
+            const double f0 = hermite_z(z0, o[5], z1, n[5], dt, left) - zs;
+            const double f1 = hermite_z(z0, o[5], z1, n[5], dt, right) - zs;
+            if (!(right > left) || f0 == 0.0 || sgn(f0) == sgn(f1)) continue;
+            double lo = left, hi = right, flo = f0;
+            for (int it = 0; it < 60; ++it) {
+                const double mid = 0.5 * (lo + hi);
+                const double fm = hermite_z(z0, o[5], z1, n[5], dt, mid) - zs;
+                const bool same = sgn(fm) == sgn(flo);
+                if (same) { lo = mid; flo = fm; } else { hi = mid; }
+            }
+            const double sv = 0.5 * (lo + hi);
+            const double s2 = sv * sv, s3 = s2 * sv;
+            const double h00 = 2 * s3 - 3 * s2 + 1, h10 = s3 - 2 * s2 + sv, h01 = -2 * s3 + 3 * s2, h11 = s3 - s2;
+            const double d00 = 6 * s2 - 6 * sv, d10 = 3 * s2 - 4 * sv + 1, d01 = -6 * s2 + 6 * sv, d11 = 3 * s2 - 2 * sv;
+            const unsigned long long slot = atomicAdd(prm.screen_count, 1ull);
+            if ((long long)slot >= prm.screen_capacity) continue;
+            const long long cap = prm.screen_capacity;
+            double* r = prm.screen_rec;
+            r[0 * cap + slot] = t_old + sv * dt;
+            for (int k = 0; k < 3; ++k) {
+                r[(1 + k) * cap + slot] = h00 * o[k] + (h10 * dt) * o[3 + k] + h01 * n[k] + (h11 * dt) * n[3 + k];
+                r[(4 + k) * cap + slot] = (d00 / dt) * o[k] + d10 * o[3 + k] + (d01 / dt) * n[k] + d11 * n[3 + k];
+            }
+            r[7 * cap + slot] = (double)sidx;
+            r[8 * cap + slot] = (double)particle;
+        }
+    }
+}
+
+__device__ __forceinline__ void write_output(const SptTraceParams& prm, long long n_particles, int k, long long pidx,
+                                             double t, const double* s) {
+    double* r = prm.output_rec + (size_t)k * 7 * n_particles;
+    r[pidx] = t;
+    for (int c = 0; c < 6; ++c) r[(size_t)(1 + c) * n_particles + pidx] = s[c];
+    prm.output_flag[(size_t)k * n_particles + pidx] = 1;
+}
 
 template <int KIND>
 __global__ void __launch_bounds__(kThreads, 1)
@@ -844,12 +932,28 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
             c.cps[r] = v;
         }
         __syncthreads();
-        if (tid == 0 && gs.status == SPT_GROUP_NEW) {
-            gs.t = c.cps[0];
-            gs.h = (prm.t_max - gs.t) * prm.initial_step_fraction;
-            gs.status = SPT_GROUP_RUNNING;
+        if (tid == 0) {
+            gs.fire_out = -1;
+            if (gs.status == SPT_GROUP_NEW) {
+                gs.t = c.cps[0];
+                gs.h = (prm.t_max - gs.t) * prm.initial_step_fraction;
+                gs.status = SPT_GROUP_RUNNING;
+                // an output time equal to the start time fires here (batched_rk45.py:191-209)
+                if (prm.n_outputs > 0) {
+                    const int last = count_le(prm.output_times, prm.n_outputs, gs.t) - 1;
+                    if (last >= 0 && prm.output_times[last] == gs.t) gs.fire_out = last;
+                }
+            }
         }
         __syncthreads();
+        if (gs.fire_out >= 0) {
+            for (int i = tid; i < E; i += kThreads) {
+                if (c.tb[i] <= gs.t) {
+                    const double sv[6] = {y0[0][i], y0[1][i], y0[2][i], y0[3][i], y0[4][i], y0[5][i]};
+                    write_output(prm, st.n_particles, gs.fire_out, base + i, gs.t, sv);
+                }
+            }
+        }
         double* kp[7]; double* kv[7];
         for (int s = 0; s < 7; ++s) { kp[s] = c.kp + 3 * s * Emax; kv[s] = c.kv + 3 * s * Emax; }
         // The stage routines index slope arrays as out[comp*E + i] with the group's E.
@@ -861,7 +965,14 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
                 while (lo < hi) { const int mid = (lo + hi) >> 1; if (c.cps[mid] <= gs.t) lo = mid + 1; else hi = mid; }
                 gs.exhausted = lo >= E;
                 gs.next_cp = gs.exhausted ? prm.t_max : c.cps[lo];
-                const double target = fmin(gs.next_cp, prm.t_max);
+                double target = fmin(gs.next_cp, prm.t_max);
+                if (prm.n_outputs > 0) {
+                    const int optr = count_le(prm.output_times, prm.n_outputs, gs.t);
+                    gs.out_ptr = optr;
+                    gs.out_exh = optr >= prm.n_outputs;
+                    gs.next_out = gs.out_exh ? prm.t_max : prm.output_times[optr];
+                    target = fmin(target, gs.next_out);
+                }
                 gs.hr = fmin(gs.h, target - gs.t);
                 if (!(gs.hr > 0.0) || !isfinite(gs.hr)) gs.status = SPT_GROUP_NONFINITE;
             }
@@ -953,10 +1064,17 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
             __syncthreads();
             if (gs.accepted) {
                 const double t_new = t + hr;
+                const double dt = t_new - t;
+                const double tol_out = 1e-9 * fmax(prm.t_max, 1e-30);
+                const bool hit = prm.n_outputs > 0 && !gs.out_exh && t_new >= gs.next_out - tol_out;
                 for (int i = tid; i < E; i += kThreads) {
                     const bool was = c.live[i];
-                    for (int k = 0; k < 6; ++k) y0[k][i] = nw[k][i];
                     if (was && kill_test<KIND>(nw[0][i], nw[1][i], nw[2][i], geo)) c.td[i] = t_new;
+                    double o[6], nv[6];
+                    for (int k = 0; k < 6; ++k) { o[k] = y0[k][i]; nv[k] = nw[k][i]; }
+                    if (hit && c.tb[i] <= t_new) write_output(prm, st.n_particles, gs.out_ptr, base + i, t_new, nv);
+                    if (prm.n_screens > 0) screen_crossings(prm, o, nv, t, dt, base + i);
+                    for (int k = 0; k < 6; ++k) y0[k][i] = nv[k];
                 }
                 if (tid == 0) {
                     gs.t = t_new;

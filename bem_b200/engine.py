@@ -120,7 +120,7 @@ class Tracer:
 
     def params(self, t_max, rtol, atol, plummer_radius, charge_to_mass, max_attempts, log=None,
                safety=0.9, min_factor=0.2, max_factor=10.0, initial_step_fraction=1e-6,
-               coulomb_constant=COULOMB_CONSTANT):
+               coulomb_constant=COULOMB_CONSTANT, records=None):
         p = _lib.SptTraceParams()
         p.t_max, p.rtol, p.atol = float(t_max), float(rtol), float(atol)
         p.plummer_radius = float(plummer_radius)
@@ -135,6 +135,8 @@ class Tracer:
             p.log_h = log[0].data_ptr()
             p.log_err = log[1].data_ptr()
         p.counters = self.counters.data_ptr()
+        if records is not None:
+            records.fill(p)
         return p
 
     def workspace(self, state, params):
@@ -162,10 +164,19 @@ class Tracer:
                                         ctypes.c_void_p(stream.cuda_stream)), "spt_trace")
 
     def run(self, batch, t_max, rtol, atol, plummer_radius, charge_to_mass, max_steps=10_000_000,
-            attempt_chunk=DEFAULT_ATTEMPT_CHUNK, log_capacity=0, **kw):
+            attempt_chunk=DEFAULT_ATTEMPT_CHUNK, log_capacity=0, screens=None, output_times=None,
+            screen_capacity=None, **kw):
         """Integrate every group to t_max.  Raises RuntimeError when a group
-        needs more than max_steps attempts (batched_rk45.py:320-321)."""
+        needs more than max_steps attempts (batched_rk45.py:320-321).
+
+        With `screens` (z planes) and/or `output_times`, returns a
+        TraceRecords holding every crossing and every output-time snapshot;
+        otherwise returns the attempt log (or None)."""
         torch = _torch()
+        records = None
+        if screens or output_times is not None:
+            records = TraceRecords(batch, screens or [], output_times, self.device, screen_capacity)
+            kw["records"] = records
         log = None
         if log_capacity:
             log = (torch.full((batch.n_groups, log_capacity), float("nan"), dtype=torch.float64, device=self.device),
@@ -178,6 +189,8 @@ class Tracer:
             p = self.params(t_max, rtol, atol, plummer_radius, charge_to_mass, chunk, log=log, **kw)
             self.launch(batch, p)
             done_attempts += chunk
+            if records is not None:
+                records.collect()
             status = batch.status.cpu().numpy()
             bad = np.isin(status, [_lib.GROUP_NONFINITE, _lib.GROUP_TIMEOUT])
             if np.any(bad):
@@ -186,11 +199,91 @@ class Tracer:
                                    f"({'non-finite error norm' if status[g] == _lib.GROUP_NONFINITE else 'device wait timeout'})")
             if np.all(status == _lib.GROUP_DONE):
                 break
-        return log
+        return records if records is not None else log
 
     def counter_dict(self):
         c = self.counters.cpu().numpy().astype(np.uint64)
         return {k: int(v) for k, v in zip(_lib.COUNTERS, c)}
+
+
+class TraceRecords:
+    """Device buffers for screen crossings and output-time snapshots, and
+    their host copies (screens.py:18-40, trajectories.py:16-41)."""
+
+    def __init__(self, batch, screens, output_times, device, screen_capacity=None):
+        torch = _torch()
+        self.batch = batch
+        self.screens = [float(z) for z in screens]
+        n = batch.n_particles
+        ns = len(self.screens)
+        self.capacity = int(screen_capacity or (8 * n * max(ns, 1) + 4096))
+        f64 = torch.float64
+        self.screen_z = torch.as_tensor(np.asarray(self.screens, dtype=np.float64), device=device) if ns else None
+        self.screen_rec = torch.empty((9, self.capacity), dtype=f64, device=device) if ns else None
+        self.screen_count = torch.zeros(1, dtype=torch.int64, device=device)
+        self.chunks = []
+        if output_times is not None:
+            self.output_times = np.sort(np.asarray(output_times, dtype=np.float64))
+            no = len(self.output_times)
+            self.out_t = torch.as_tensor(self.output_times, device=device)
+            self.out_rec = torch.zeros((no, 7, n), dtype=f64, device=device)
+            self.out_flag = torch.zeros((no, n), dtype=torch.uint8, device=device)
+        else:
+            self.output_times = None
+
+    def fill(self, p):
+        if self.screens:
+            p.n_screens = len(self.screens)
+            p.screens = self.screen_z.data_ptr()
+            p.screen_rec = self.screen_rec.data_ptr()
+            p.screen_capacity = self.capacity
+            p.screen_count = self.screen_count.data_ptr()
+        if self.output_times is not None and len(self.output_times):
+            p.n_outputs = len(self.output_times)
+            p.output_times = self.out_t.data_ptr()
+            p.output_rec = self.out_rec.data_ptr()
+            p.output_flag = self.out_flag.data_ptr()
+
+    def collect(self):
+        """Move this launch's crossings to the host and reset the counter."""
+        if not self.screens:
+            return
+        n = int(self.screen_count.item())
+        if n > self.capacity:
+            raise RuntimeError(f"{n} screen crossings in one launch exceed the record buffer ({self.capacity}); "
+                               "pass a larger screen_capacity")
+        if n:
+            self.chunks.append(self.screen_rec[:, :n].cpu().numpy())
+        self.screen_count.zero_()
+
+    def screen_records(self):
+        """One dict of arrays per screen, in the order found (or None)."""
+        allr = np.concatenate(self.chunks, axis=1) if self.chunks else np.zeros((9, 0))
+        out = []
+        for k in range(len(self.screens)):
+            r = allr[:, allr[7] == k]
+            if r.shape[1] == 0:
+                out.append(None)
+                continue
+            out.append(dict(t=r[0], x=r[1], y=r[2], z=r[3], vx=r[4], vy=r[5], vz=r[6],
+                            particle=r[8].astype(np.int64)))
+        return out
+
+    def output_records(self):
+        """One dict of arrays per output time: every particle born by then."""
+        if self.output_times is None:
+            return []
+        rec = self.out_rec.cpu().numpy()
+        flag = self.out_flag.cpu().numpy().astype(bool)
+        out = []
+        for k in range(len(self.output_times)):
+            idx = np.nonzero(flag[k])[0]
+            if len(idx) == 0:
+                out.append(None)
+                continue
+            r = rec[k][:, idx]
+            out.append(dict(t=r[0], x=r[1], y=r[2], z=r[3], vx=r[4], vy=r[5], vz=r[6], particle=idx))
+        return out
 
 
 def accel(geometry, pos, active, charge, mass, group_sizes, charge_to_mass, plummer_radius, device="cuda",

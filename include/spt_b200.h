@@ -144,6 +144,26 @@ typedef struct {
     double* log_h;                 /* [n_groups][log_capacity] step used by attempt k */
     double* log_err;               /* [n_groups][log_capacity] its error norm */
     unsigned long long* counters;  /* [SPT_N_COUNTERS] or NULL */
+    /* screens (screens.py:43-168): z planes; every crossing inside an accepted
+     * step is located on the step's cubic Hermite z(s) (split at its extrema,
+     * 60 bisection steps) and appended to screen_rec, a [9][screen_capacity]
+     * array of (t, x, y, z, vx, vy, vz, screen index, particle index);
+     * screen_count counts every crossing found, including any beyond the
+     * capacity (which are dropped). */
+    int32_t n_screens;
+    int32_t n_outputs;
+    const double* screens;
+    double* screen_rec;
+    int64_t screen_capacity;
+    unsigned long long* screen_count;
+    /* output times (batched_rk45.py:186-209, 295-312; trajectories.py:44-74):
+     * ascending; every group's step lands on each one exactly; the state of
+     * every particle born by then is written to output_rec
+     * [n_outputs][7][n_particles] (t, x, y, z, vx, vy, vz) and flagged in
+     * output_flag [n_outputs][n_particles]. */
+    const double* output_times;
+    double* output_rec;
+    uint8_t* output_flag;
 } SptTraceParams;
 
 /* Scratch bytes spt_trace needs for this state/geometry (work-queue
