@@ -333,7 +333,7 @@ __device__ __forceinline__ bool seg_near(const SptBem& b, int s, double re, doub
 // node table streams through shared memory in TMA tiles (double buffered);
 // each thread takes NQ nodes at a time, strided by the CTA width, against
 // all NP points (NP * NQ independent ring evaluations per iteration).
-template <int NP, int NQ>
+template <int NP, int NQ, bool MIX>
 __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_tile, bool& ok,
                           unsigned long long& far_evals) {
     const SptBem& b = c.bem;
@@ -344,6 +344,7 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
     double* tile[2] = {c.tiles, c.tiles + 3 * tile_cap};
     uint64_t* bars = c.bars;
     double pr[NP], pinv[NP], pz[NP], ar[NP], az[NP];
+    float fr[NP], fz[NP], kr[NP], kz[NP], prf[NP], pinvf[NP];  // mixed form: Kahan sums and float copies
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
         const int k = r0 + (p < np_ ? p : 0);
@@ -352,6 +353,9 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
         pz[p] = P[8 * k + 4];
         ar[p] = 0.0;
         az[p] = 0.0;
+        fr[p] = fz[p] = kr[p] = kz[p] = 0.0f;
+        prf[p] = (float)pr[p];
+        pinvf[p] = (float)pinv[p];
     }
     auto issue = [&](int t, int buf) {
         const int s_first = t * segs_per_tile;
@@ -397,18 +401,46 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
                     wq[j] = tw[qq];
                     sl[j] = qq / nps;
                 }
+                if (MIX) {
+                    // float32 Kahan sums; pairs the float path declines (p < 1e-3 or
+                    // near the axis) are evaluated in float64
+#pragma unroll
+                    for (int p = 0; p < NP; ++p) {
+#pragma unroll
+                        for (int j = 0; j < NQ; ++j) {
+                            if (p < np_ && in[j] && !c.nflag[p * 256 + sl[j]]) {
+                                const double dz = pz[p] - zq[j];
+                                float er, ez;
+                                if (ring_far_f(prf[p], pinvf[p], (float)(pr[p] - rq[j]), (float)(pr[p] + rq[j]),
+                                               (float)dz, (float)rq[j], er, ez)) {
+                                    const float w = (float)wq[j];
+                                    kahan_add(fr[p], kr[p], w * er);
+                                    kahan_add(fz[p], kz[p], w * ez);
+                                } else {
+                                    double e64r, e64z;
+                                    ring_field_far(pr[p], pinv[p], dz, rq[j], e64r, e64z);
+                                    ar[p] = fma(wq[j], e64r, ar[p]);
+                                    az[p] = fma(wq[j], e64z, az[p]);
+                                }
+                                ++far_evals;
+                            }
+                        }
+                    }
+                } else {
 #pragma unroll
                 for (int p = 0; p < NP; ++p) {
 #pragma unroll
                     for (int j = 0; j < NQ; ++j) {
                         if (p < np_ && in[j] && !c.nflag[p * 256 + sl[j]]) {
+                            const double dz = pz[p] - zq[j];
                             double er, ez;
-                            ring_field_far(pr[p], pinv[p], pz[p] - zq[j], rq[j], er, ez);
+                            ring_field_far(pr[p], pinv[p], dz, rq[j], er, ez);
                             ar[p] = fma(wq[j], er, ar[p]);
                             az[p] = fma(wq[j], ez, az[p]);
                             ++far_evals;
                         }
                     }
+                }
                 }
             }
         }
@@ -418,6 +450,10 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
     // fixed-order block reduction of the round's accumulators
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
+        if (MIX) {
+            ar[p] += (double)fr[p] - (double)kr[p];
+            az[p] += (double)fz[p] - (double)kz[p];
+        }
         const double vr = warp_sum(ar[p]);
         const double vz = warp_sum(az[p]);
         if (lane == 0) {
@@ -539,14 +575,25 @@ __device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
     bool ok = true;
     for (int r0 = 0; r0 < n; r0 += kRound) {
         const int np_ = min(kRound, n - r0);
-        if (np_ == 1)
-            far_round<1, 8>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-        else if (np_ == 2)
-            far_round<2, 4>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-        else if (np_ <= 4)
-            far_round<4, 2>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-        else
-            far_round<8, 1>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+        if (c.form == SPT_FORM_MIXED) {
+            if (np_ == 1)
+                far_round<1, 8, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+            else if (np_ == 2)
+                far_round<2, 4, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+            else if (np_ <= 4)
+                far_round<4, 2, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+            else
+                far_round<8, 1, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+        } else {
+            if (np_ == 1)
+                far_round<1, 8, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+            else if (np_ == 2)
+                far_round<2, 4, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+            else if (np_ <= 4)
+                far_round<4, 2, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+            else
+                far_round<8, 1, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+        }
     }
     if (!ok && tid == 0) *status_flag = SPT_GROUP_TIMEOUT;
     c.cnt[SPT_CNT_RING_FAR] += far_evals;
@@ -572,6 +619,50 @@ __device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
         }
     }
     __syncthreads();
+}
+
+// Softened pair sum over the live sources of the group (forces.py:16-29):
+// sum_j k q_i q_j (r_i - r_j) / (|r_i - r_j|^2 + a^2)^1.5, sources given by
+// src(j, x, y, z, q).  float64: the reference's operation order.  Mixed
+// form: separations are taken in float64 (nearby particles far from the
+// origin), then the rest in float32 with Kahan-compensated sums.
+template <bool MIX, typename SRC>
+__device__ __forceinline__ void pair_sum(const Ctx& c, int E, double xi, double yi, double zi, double qk, SRC src,
+                                         double& fx, double& fy, double& fz) {
+    if (!MIX) {
+        double ax = 0.0, ay = 0.0, az = 0.0;
+        for (int j = 0; j < E; ++j) {
+            if (!c.live[j]) continue;
+            double x, y, z, q;
+            src(j, x, y, z, q);
+            const double dx = xi - x, dy = yi - y, dz = zi - z;
+            const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
+            const double r3 = r2 * sqrt(r2);
+            const double cf = qk * q / r3;
+            ax = fma(cf, dx, ax);
+            ay = fma(cf, dy, ay);
+            az = fma(cf, dz, az);
+        }
+        fx = ax; fy = ay; fz = az;
+    } else {
+        float ax = 0.f, ay = 0.f, az = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+        const float soft2 = (float)c.soft2;
+        for (int j = 0; j < E; ++j) {
+            if (!c.live[j]) continue;
+            double x, y, z, q;
+            src(j, x, y, z, q);
+            const float dx = (float)(xi - x), dy = (float)(yi - y), dz = (float)(zi - z);
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
+            const float rs = rsqrtf(r2);
+            const float cf = (float)(qk * q) * (rs * rs * rs);
+            kahan_add(ax, cx, cf * dx);
+            kahan_add(ay, cy, cf * dy);
+            kahan_add(az, cz, cf * dz);
+        }
+        fx = (double)ax - (double)cx;
+        fy = (double)ay - (double)cy;
+        fz = (double)az - (double)cz;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -678,61 +769,47 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
                 ez = w * nz + (1.0 - w) * fz;
             }
             const double qk = c.kc * c.q[i];
+            const bool mix = c.form == SPT_FORM_MIXED;
             double fcx = 0.0, fcy = 0.0, fcz = 0.0;
             if (E > 1) {
-                for (int j = 0; j < E; ++j) {
-                    if (!c.live[j]) continue;
-                    const double dx = xi - sx[j], dy = yi - sy[j], dz = zi - sz[j];
-                    const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
-                    const double r3 = r2 * sqrt(r2);
-                    const double cf = qk * c.q[j] / r3;
-                    fcx = fma(cf, dx, fcx);
-                    fcy = fma(cf, dy, fcy);
-                    fcz = fma(cf, dz, fcz);
-                }
+                auto real = [&](int j, double& x, double& y, double& z, double& q) {
+                    x = sx[j]; y = sy[j]; z = sz[j]; q = c.q[j];
+                };
+                if (mix) pair_sum<true>(c, E, xi, yi, zi, qk, real, fcx, fcy, fcz);
+                else pair_sum<false>(c, E, xi, yi, zi, qk, real, fcx, fcy, fcz);
                 pairs += E;
             }
             double fix = 0.0, fiy = 0.0, fiz = 0.0;
             if (KIND == SPT_GEOM_FLAT && g.has_image) {
                 const double zimg = -2.0 * g.z0;
-                for (int j = 0; j < E; ++j) {
-                    if (!c.live[j]) continue;
-                    const double dx = xi - sx[j], dy = yi - sy[j], dz = zi - (zimg - sz[j]);
-                    const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
-                    const double r3 = r2 * sqrt(r2);
-                    const double cf = qk * (-c.q[j]) / r3;
-                    fix = fma(cf, dx, fix);
-                    fiy = fma(cf, dy, fiy);
-                    fiz = fma(cf, dz, fiz);
-                }
+                auto mirror = [&](int j, double& x, double& y, double& z, double& q) {
+                    x = sx[j]; y = sy[j]; z = zimg - sz[j]; q = -c.q[j];
+                };
+                if (mix) pair_sum<true>(c, E, xi, yi, zi, qk, mirror, fix, fiy, fiz);
+                else pair_sum<false>(c, E, xi, yi, zi, qk, mirror, fix, fiy, fiz);
                 pairs += E;
             } else if (three_img) {
                 const double zc = (KIND == SPT_GEOM_POST_BEM) ? g.L : 0.0;
                 const double pz0 = (KIND == SPT_GEOM_POST_BEM) ? g.L + g.z0 : g.z0;
                 const double zl = zi - zc;
-                double s1x = 0, s1y = 0, s1z = 0, s2x = 0, s2y = 0, s2z = 0, s3x = 0, s3y = 0, s3z = 0;
-                for (int j = 0; j < E; ++j) {
-                    if (!c.live[j]) continue;
-                    const double qj = c.q[j];
-                    const double ix = c.img[j], iy = c.img[E + j], iz = c.img[2 * E + j], iq = c.img[3 * E + j];
-                    {   // sphere image
-                        const double dx = xi - ix, dy = yi - iy, dz = zl - iz;
-                        const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
-                        const double cf = qk * iq / (r2 * sqrt(r2));
-                        s1x = fma(cf, dx, s1x); s1y = fma(cf, dy, s1y); s1z = fma(cf, dz, s1z);
-                    }
-                    {   // plane image
-                        const double dx = xi - sx[j], dy = yi - sy[j], dz = zl - (-2.0 * pz0 - (sz[j] - zc));
-                        const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
-                        const double cf = qk * (-qj) / (r2 * sqrt(r2));
-                        s2x = fma(cf, dx, s2x); s2y = fma(cf, dy, s2y); s2z = fma(cf, dz, s2z);
-                    }
-                    {   // plane image of the sphere image
-                        const double dx = xi - ix, dy = yi - iy, dz = zl - (-2.0 * pz0 - iz);
-                        const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
-                        const double cf = qk * (-iq) / (r2 * sqrt(r2));
-                        s3x = fma(cf, dx, s3x); s3y = fma(cf, dy, s3y); s3z = fma(cf, dz, s3z);
-                    }
+                double s1x, s1y, s1z, s2x, s2y, s2z, s3x, s3y, s3z;
+                auto sphere = [&](int j, double& x, double& y, double& z, double& q) {
+                    x = c.img[j]; y = c.img[E + j]; z = c.img[2 * E + j]; q = c.img[3 * E + j];
+                };
+                auto plane = [&](int j, double& x, double& y, double& z, double& q) {
+                    x = sx[j]; y = sy[j]; z = -2.0 * pz0 - (sz[j] - zc); q = -c.q[j];
+                };
+                auto plane_sphere = [&](int j, double& x, double& y, double& z, double& q) {
+                    x = c.img[j]; y = c.img[E + j]; z = -2.0 * pz0 - c.img[2 * E + j]; q = -c.img[3 * E + j];
+                };
+                if (mix) {
+                    pair_sum<true>(c, E, xi, yi, zl, qk, sphere, s1x, s1y, s1z);
+                    pair_sum<true>(c, E, xi, yi, zl, qk, plane, s2x, s2y, s2z);
+                    pair_sum<true>(c, E, xi, yi, zl, qk, plane_sphere, s3x, s3y, s3z);
+                } else {
+                    pair_sum<false>(c, E, xi, yi, zl, qk, sphere, s1x, s1y, s1z);
+                    pair_sum<false>(c, E, xi, yi, zl, qk, plane, s2x, s2y, s2z);
+                    pair_sum<false>(c, E, xi, yi, zl, qk, plane_sphere, s3x, s3y, s3z);
                 }
                 fix = (s1x + s2x) + s3x;
                 fiy = (s1y + s2y) + s3y;
@@ -1163,12 +1240,13 @@ accel_kernel(SptAccelArgs a, SptGeometry geo, SptBem bem) {
 // BEM perturbation field at arbitrary points (spt_bem_field): kRound*8 points per CTA
 constexpr int kFieldChunk = 64;
 __global__ void __launch_bounds__(kThreads, 1)
-bem_field_kernel(const double* x, const double* y, const double* z, long long n, SptBem bem, double* ex, double* ey,
-                 double* ez, unsigned long long* counters) {
+bem_field_kernel(const double* x, const double* y, const double* z, long long n, SptBem bem, int form, double* ex,
+                 double* ey, double* ez, unsigned long long* counters) {
     extern __shared__ __align__(16) double smem[];
     __shared__ int s_flag;
     Ctx c;
     c.bem = bem;
+    c.form = form;
     bind(c, smem, kFieldChunk, nullptr);
     init_barriers(c);
     const long long p0 = (long long)blockIdx.x * kFieldChunk;
@@ -1437,14 +1515,14 @@ int spt_bem_field(const double* x, const double* y, const double* z, int64_t n, 
     if (!x || !y || !z || !ex || !ey || !ez) return fail(SPT_ERR_ARG, "null argument");
     int rc = check_bem(b);
     if (rc) return rc;
-    (void)form;
+    if (form != SPT_FORM_FP64 && form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "unknown form %d", form);
     const spt::Layout L = spt::make_layout(spt::kFieldChunk, true);
     rc = set_smem(spt::bem_field_kernel, L.bytes);
     if (rc) return rc;
     const long long blocks = (n + spt::kFieldChunk - 1) / spt::kFieldChunk;
     if (blocks > 0x7fffffffLL) return fail(SPT_ERR_CAPACITY, "too many points");
     spt::bem_field_kernel<<<(unsigned)blocks, spt::kThreads, L.bytes, static_cast<cudaStream_t>(stream)>>>(
-        x, y, z, n, *b, ex, ey, ez, nullptr);
+        x, y, z, n, *b, form, ex, ey, ez, nullptr);
     return cuda_check(cudaGetLastError(), "bem_field_kernel launch");
 }
 

@@ -197,4 +197,82 @@ __device__ __forceinline__ void ring_field_f(float rho, float z, float a, float&
     ez = z * E * rsD * inv_d2 * (1.0f / (2.0f * 9.8696044f));
 }
 
+
+// float32 K, E for the far sum of the mixed form: the 4-term DLMF 19.12
+// series below p = 1e-2, a fixed five-step AGM above (for p >= 1e-2 the fifth
+// half-difference is below 1e-9, so a_5 has converged to float precision).
+// Callers send p < 1e-3 to the float64 path instead.
+__device__ __forceinline__ void ellip_ke_f_fixed(float p, float& K, float& E) {
+    if (p < 1e-2f) {
+        const float L = -0.5f * __logf(p);
+        const float A = fmaf(fmaf(fmaf(0.09765625f, p, 0.140625f), p, 0.25f), p, 1.0f);
+        const float B = fmaf(fmaf(fmaf(0.01493760037f, p, 0.03088514453f), p, 0.09657359028f), p, 1.386294361f);
+        const float C = fmaf(fmaf(fmaf(0.1708984375f, p, 0.234375f), p, 0.375f), p, 1.0f);
+        const float D = fmaf(fmaf(fmaf(0.02308904283f, p, 0.04366274089f), p, 0.1136103854f), p, 0.8862943611f);
+        K = fmaf(L, A, B);
+        E = fmaf(0.5f * p, fmaf(L, C, D), 1.0f);
+        return;
+    }
+    float a = 1.0f, b = p * rsqrtf(p);
+    float S = 0.5f * (1.0f - p), w = 0.5f;
+#pragma unroll
+    for (int it = 0; it < 5; ++it) {
+        const float c = 0.5f * (a - b);
+        const float an = 0.5f * (a + b);
+        const float ab = a * b;
+        b = ab * rsqrtf(ab);
+        a = an;
+        w += w;
+        S = fmaf(w * c, c, S);
+    }
+    K = 1.5707963267948966f * __frcp_rn(a);
+    E = K * (1.0f - S);
+}
+
+// float32 ring field for the far sum of the mixed form, branch free so that
+// several evaluations interleave.  dr = rho - a and sr = rho + a are formed in
+// float64 by the caller (rho and a are close near a wall), then rounded.
+// K and E come from a fixed six-step float AGM (converged for p >= 1e-3).
+// Returns false -- the caller then uses the float64 ring_field_far -- when
+// p = d2/D < 1e-3 (m > 0.999, where K(m -> 1) needs the digits) or when the
+// point is within 1e-2 of the node distance from the axis (the radial
+// component cancels there and is scaled by 1/rho; the Taylor branch needs
+// (a^2+z^2)^-3.5, beyond float range for nm rings).
+__device__ __forceinline__ bool ring_far_f(float rho, float inv_rho, float dr, float sr, float z, float a, float& er,
+                                           float& ez) {
+    const float z2 = z * z, a2 = a * a, rho2 = rho * rho;
+    const float D = fmaf(sr, sr, z2);
+    const float d2 = fmaf(dr, dr, z2);
+    const float invD = __frcp_rn(D);
+    const float p = d2 * invD;
+    const bool ok = (p >= 1e-3f) && (rho2 >= 1e-4f * (a2 + z2));
+    const float pc = fmaxf(p, 1e-3f);
+    float aa = 1.0f, bb = pc * rsqrtf(pc);
+    float S = 0.5f * (1.0f - pc), w = 0.5f;
+#pragma unroll
+    for (int it = 0; it < 6; ++it) {
+        const float c = 0.5f * (aa - bb);
+        const float an = 0.5f * (aa + bb);
+        const float ab = aa * bb;
+        bb = ab * rsqrtf(ab);
+        aa = an;
+        w += w;
+        S = fmaf(w * c, c, S);
+    }
+    const float K = 1.5707963267948966f * __frcp_rn(aa);
+    const float E = K * (1.0f - S);
+    const float inv_d2 = __frcp_rn(d2);
+    const float rsD = rsqrtf(D);
+    er = (K - (a2 - rho2 + z2) * E * inv_d2) * (rsD * inv_rho * 0.025330295910584444f);  // 1/(4 pi^2)
+    ez = z * E * rsD * inv_d2 * 0.05066059182116889f;                                    // 1/(2 pi^2)
+    return ok;
+}
+
+__device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
+    const float y = v - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
+}
+
 }  // namespace spt
