@@ -62,6 +62,16 @@ class SptAccelArgs(ctypes.Structure):
                 ("ax", _p), ("ay", _p), ("az", _p)]
 
 
+class SptGemmArgs(ctypes.Structure):
+    _fields_ = [("M", _i32), ("N", _i32), ("K", _i32), ("a_mn", _i32), ("b_mn", _i32), ("epi", _i32),
+                ("split_k", _i32), ("reserved", _i32), ("lda", _i64), ("ldb", _i64), ("ldc", _i64),
+                ("split_stride", _i64), ("A", _p), ("B", _p), ("C", _p), ("bias", _p), ("Z", _p), ("H", _p),
+                ("status", _p)]
+
+
+EPI_STORE, EPI_BIAS_SILU, EPI_DSILU = 0, 1, 2
+_f = ctypes.c_float
+
 # entry point -> (restype, argtypes)
 SIGNATURES = {
     "spt_abi_version": (ctypes.c_int, []),
@@ -77,6 +87,12 @@ SIGNATURES = {
     "spt_ring_field": (ctypes.c_int, [_p, _p, _p, _i64, _i32, _p, _p, _p]),
     "spt_ellip_ke": (ctypes.c_int, [_p, _i64, _i32, _p, _p, _p]),
     "spt_bem_assemble": (ctypes.c_int, [_p, _p, _i32, _d, _i32, _p, _p, _p, _p]),
+    "spt_mlp_gemm": (ctypes.c_int, [ctypes.POINTER(SptGemmArgs), _p]),
+    "spt_mlp_first_layer": (ctypes.c_int, [_p, _i64, _p, _p, _p, _p, _p]),
+    "spt_mlp_last_layer": (ctypes.c_int, [_p, _p, _i64, _p, _p, _p, _p, _f, _p, _p, _p, _p, _p]),
+    "spt_mlp_colsum": (ctypes.c_int, [_p, _i64, _p, _p, _p, _p]),
+    "spt_mlp_reduce_splits": (ctypes.c_int, [_p, _i32, _i64, _p, _p]),
+    "spt_mlp_adam": (ctypes.c_int, [_p, _p, _p, _p, _i64, _f, _f, _f, _f, _i32, _p, _p, _p]),
     "spt_trace_noalloc": (ctypes.c_int, [ctypes.POINTER(SptState), ctypes.POINTER(SptTraceParams),
                                          ctypes.POINTER(SptGeometry), ctypes.POINTER(SptBem), _p]),
 }

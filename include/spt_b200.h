@@ -243,6 +243,35 @@ int spt_bem_assemble(const double* profile_rho, const double* profile_z, int32_t
 int spt_trace_noalloc(const SptState* state, const SptTraceParams* params, const SptGeometry* geom,
                       const SptBem* bem, void* stream);
 
+/* ---- learned field surrogate: BF16 tensor-core MLP kernels (no counterpart
+ * in the reference; they train and evaluate the (rho, z) -> (E_rho, E_z)
+ * surrogate of the BEM field).  Return 0, 1 (bad argument) or 2 (launch). */
+#define SPT_EPI_STORE 0       /* C = acc (FP32), per K split at C + split * split_stride */
+#define SPT_EPI_BIAS_SILU 1   /* C = z = acc + bias (FP32, optional), H = SiLU(z) (BF16) */
+#define SPT_EPI_DSILU 2       /* H = acc * SiLU'(Z) (BF16) */
+typedef struct {
+    int32_t M, N, K;          /* D[M x N] = A[M x K] B[N x K]^T; K a multiple of 64 (of 64 * split_k) */
+    int32_t a_mn, b_mn;       /* 0: element (r, k) at X[r*ld + k]; 1: at X[k*ld + r] */
+    int32_t epi, split_k, reserved;
+    int64_t lda, ldb, ldc, split_stride;   /* lda, ldb multiples of 8 */
+    const void* A;            /* BF16, 16-byte aligned */
+    const void* B;            /* BF16, 16-byte aligned */
+    float* C;
+    const float* bias;
+    const float* Z;
+    void* H;                  /* BF16 */
+    int32_t* status;          /* set to 1 if a bounded wait gave up (optional) */
+} SptGemmArgs;
+int spt_mlp_gemm(const SptGemmArgs* args, void* stream);
+int spt_mlp_first_layer(const float* x, int64_t n, const float* W1, const float* b1, float* z, void* h, void* stream);
+int spt_mlp_last_layer(const void* h, const float* z, int64_t n, const float* W5, const float* b5, float* y,
+                       const float* target, float inv_batch, void* delta, float* dW5, float* db5, float* loss,
+                       void* stream);
+int spt_mlp_colsum(const void* delta, int64_t n, const float* x, float* db, float* dW1, void* stream);
+int spt_mlp_reduce_splits(const float* part, int32_t splits, int64_t n, float* out, void* stream);
+int spt_mlp_adam(float* p, const float* g, float* m, float* v, int64_t n, float lr, float beta1, float beta2,
+                 float eps, int32_t step, void* p_bf16, float* p_rounded, void* stream);
+
 /* Last error message of the calling thread (NUL-terminated, truncated to
  * len). Returns the length of the full message. */
 int spt_last_error(char* buf, int32_t len);

@@ -39,6 +39,7 @@ STRUCTS = {
     "SptState": _lib.SptState,
     "SptTraceParams": _lib.SptTraceParams,
     "SptAccelArgs": _lib.SptAccelArgs,
+    "SptGemmArgs": _lib.SptGemmArgs,
 }
 
 
