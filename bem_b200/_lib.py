@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libspt_b200.so")
 
 SPT_OK, SPT_ERR_ARG, SPT_ERR_CUDA, SPT_ERR_CAPACITY = 0, 1, 2, 3
 GEOM_FLAT, GEOM_TIP, GEOM_TIP_BEM, GEOM_WELL_BEM, GEOM_POST_BEM = 0, 1, 2, 3, 4
-FORM_FP64, FORM_MIXED = 0, 1
+FORM_FP64, FORM_MIXED, FORM_SURROGATE = 0, 1, 2
 GROUP_NEW, GROUP_RUNNING, GROUP_DONE, GROUP_NONFINITE, GROUP_TIMEOUT = 0, 1, 2, 3, 4
 COUNTERS = ("attempts", "accepted", "particle_steps", "stage_evals", "pair_evals", "ring_far", "ring_near",
             "near_pairs")
@@ -52,7 +52,9 @@ class SptTraceParams(ctypes.Structure):
                 ("log_h", _p), ("log_err", _p), ("counters", _p),
                 ("n_screens", _i32), ("n_outputs", _i32), ("screens", _p), ("screen_rec", _p),
                 ("screen_capacity", _i64), ("screen_count", _p), ("output_times", _p), ("output_rec", _p),
-                ("output_flag", _p)]
+                ("output_flag", _p), ("sur_w", _p), ("sur_w16", _p), ("sur_s_start", _p), ("sur_log_scale", _p),
+                ("sur_s_end", _d), ("sur_sig_floor", _d), ("sur_band", _d), ("sur_spot", _d), ("sur_d_min", _d),
+                ("sur_d_max", _d), ("sur_stats", _p)]
 
 
 class SptAccelArgs(ctypes.Structure):

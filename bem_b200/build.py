@@ -14,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libspt_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("spt_kernels.cu", "spt_mlp.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", "spt_math.cuh"), os.path.join(REPO, "include", "spt_b200.h")]
+DEPS = SOURCES + [os.path.join(HERE, "csrc", h) for h in ("spt_math.cuh", "spt_umma.cuh")] + [
+    os.path.join(REPO, "include", "spt_b200.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -24,6 +24,7 @@
 #include <string.h>
 
 #include "../../include/spt_b200.h"
+#include "spt_umma.cuh"
 
 namespace spt_mlp {
 
@@ -31,35 +32,18 @@ constexpr int kTile = 128;   // M and N tile
 constexpr int kChunk = 64;   // K per shared-memory chunk
 constexpr int kThreads = 128;
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+using spt_umma::dsilu;
+using spt_umma::silu;
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return spt_umma::smem_addr(p); }
+__device__ __forceinline__ uint64_t umma_desc(const void* smem, uint32_t lbo, uint32_t sbo) {
+    return spt_umma::desc(smem, lbo, sbo);
 }
-
-// UMMA shared-memory descriptor, no swizzle: start address, leading byte
-// offset (LBO) and stride byte offset (SBO) in 16-byte units, version 1.
-__device__ __forceinline__ uint64_t umma_desc(const void* smem, uint32_t lbo_bytes, uint32_t sbo_bytes) {
-    const uint64_t addr = (smem_u32(smem) >> 4) & 0x3FFFu;
-    return addr | ((uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16) | ((uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32) |
-           ((uint64_t)1 << 46);
+__host__ __device__ constexpr uint32_t umma_idesc(int a_mn, int b_mn) { return spt_umma::idesc_bf16_128(a_mn, b_mn); }
+__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t i, uint32_t acc) {
+    spt_umma::mma(d, a, b, i, acc);
 }
-
-// Instruction descriptor: D = F32, A = B = BF16, dense, M = 128, N = 128.
-__host__ __device__ constexpr uint32_t umma_idesc(int a_mn, int b_mn) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
-           ((uint32_t)(kTile >> 3) << 17) | ((uint32_t)(kTile >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-        "l"(da), "l"(db), "r"(idesc), "r"(acc));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                 : "memory");
-}
+__device__ __forceinline__ void mma_commit(uint64_t* bar) { spt_umma::commit(bar); }
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) { spt_umma::ld16(taddr, v); }
 
 __device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t phase) {
     uint32_t done = 0;
@@ -72,25 +56,6 @@ __device__ __forceinline__ bool bar_wait(uint64_t* bar, uint32_t phase) {
         if (done) return true;
     }
     return false;
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ float silu(float z) { return z / (1.0f + __expf(-z)); }
-__device__ __forceinline__ float dsilu(float z) {
-    const float s = 1.0f / (1.0f + __expf(-z));
-    return s * (1.0f + z * (1.0f - s));
 }
 
 // Copy a 128 (rows: M or N) x 64 (K) chunk of a BF16 operand into the

@@ -7,10 +7,12 @@ accumulators); the first and last layers, the loss, the bias sums and Adam
 are the library's own CUDA-core kernels.  Nothing here calls a library GEMM
 or autograd: torch only holds the buffers.
 
-Inputs are log-radial: with r the distance to the feature centre (0, zc),
-u1 = 2 (ln(r/r0) - lmin)/(lmax - lmin) - 1 and u2 = (z - zc)/r.  Outputs are
-E / S(r), S a per-log-radius RMS scale table measured on the training data,
-so every output is O(1) from the apex to z_handoff.
+Inputs are surface-normal coordinates -- the log distance to the profile
+and the arclength position of the closest profile point (the stage kernel
+finds that point anyway for the reference's on-surface rule) -- and the
+outputs are the normal and tangential field components scaled by the local
+|sigma| and a per-log-distance RMS table, so every output is O(1) from the
+surface to z_handoff.
 
 Training data: points at log-uniform distances (1 nm ... 1 mm, capped at the
 blend region) along the outward normal of uniformly chosen points of the
@@ -47,12 +49,26 @@ def _check(rc, what):
 
 class FieldSurrogate:
     """Parameters (flat FP32 master buffer + BF16 copy + BF16-rounded FP32
-    copy), feature map and output scale of the surrogate."""
+    copy) and the surface-normal frame of the surrogate.
 
-    def __init__(self, zc, r0, lmin, lmax, scale_table, device="cuda", seed=0):
+    Inputs: u1 = log distance d to the profile (normalised over
+    [D_MIN, D_MAX]) and u2 = arclength position s of the closest profile
+    point (normalised over the z >= 0 part).  Outputs: the field's components
+    along the closest segment's outward normal and unit tangent, divided by
+    (|sigma(s)| + 1e-3 max|sigma|) * g(d), g a per-log-distance RMS table."""
+
+    D_MIN, D_MAX = 1e-10, 1e-3
+
+    def __init__(self, profile, sigma, s_end, scale_table, device="cuda", seed=0):
         torch = _torch()
         self.device = torch.device(device)
-        self.zc, self.r0, self.lmin, self.lmax = float(zc), float(r0), float(lmin), float(lmax)
+        self.profile = np.asarray(profile, dtype=np.float64)
+        self.sigma = np.asarray(sigma, dtype=np.float64)
+        tan = self.profile[1:] - self.profile[:-1]
+        self.seg_len = np.linalg.norm(tan, axis=-1)
+        self.s_start = np.concatenate([[0.0], np.cumsum(self.seg_len)])[:-1]
+        self.s_end = float(s_end)
+        self.sig_floor = 1e-3 * np.abs(self.sigma).max()
         self.scale_table = np.asarray(scale_table, dtype=np.float64)
         self.offsets = {}
         o = 0
@@ -75,36 +91,77 @@ class FieldSurrogate:
         off, shape = self.offsets[name]
         return buf[off:off + int(np.prod(shape))].view(*shape)
 
-    # ---- features and scale -------------------------------------------------
-    def features(self, rho, z):
-        """(rho, z) numpy -> normalised inputs [n, 2] float32, and r."""
-        dz = z - self.zc
-        r = np.sqrt(rho * rho + dz * dz)
-        u1 = 2.0 * (np.log(np.maximum(r, 1e-300) / self.r0) - self.lmin) / (self.lmax - self.lmin) - 1.0
-        u2 = dz / np.where(r > 0, r, 1.0)
-        return np.stack([u1, u2], -1).astype(np.float32), r
+    # ---- frame, features and scale --------------------------------------------
+    def frame(self, seg):
+        tan = self.profile[seg + 1] - self.profile[seg]
+        unit = tan / self.seg_len[seg][:, None]
+        nrm = np.stack([-unit[:, 1], unit[:, 0]], -1)
+        return nrm, unit
 
-    def scale(self, r):
-        lr = np.log(np.maximum(r, 1e-300) / self.r0)
-        pos = (lr - self.lmin) / (self.lmax - self.lmin) * (N_SCALE_BINS - 1)
-        return np.exp(np.interp(pos, np.arange(N_SCALE_BINS), np.log(self.scale_table)))
+    def features(self, seg, t, d):
+        s = (self.s_start[seg] + t * self.seg_len[seg]) / self.s_end
+        ld = np.log(np.clip(d, self.D_MIN, self.D_MAX))
+        u1 = 2.0 * (ld - math.log(self.D_MIN)) / (math.log(self.D_MAX) - math.log(self.D_MIN)) - 1.0
+        u2 = 2.0 * s - 1.0
+        return np.stack([u1, u2], -1).astype(np.float32)
+
+    def log_scale_table(self):
+        return np.log(self.scale_table)
+
+    def scale(self, seg, t, d):
+        sig = np.abs(self.sigma[seg] + t * (self.sigma[seg + 1] - self.sigma[seg])) + self.sig_floor
+        ld = np.log(np.clip(d, self.D_MIN, self.D_MAX))
+        pos = (ld - math.log(self.D_MIN)) / (math.log(self.D_MAX) - math.log(self.D_MIN)) * (N_SCALE_BINS - 1)
+        g = np.exp(np.interp(pos, np.arange(N_SCALE_BINS), np.log(self.scale_table)))
+        return sig * g
+
+    def closest(self, rho, z):
+        """Closest profile segment, parameter and distance of each point
+        (bem/axisymmetric.py:341-389)."""
+        prof = self.profile
+        best = np.full(rho.shape, np.inf)
+        seg = np.zeros(rho.shape, dtype=np.int64)
+        tb = np.zeros(rho.shape)
+        for j in range(len(prof) - 1):
+            ab = prof[j + 1] - prof[j]
+            t = np.clip(((rho - prof[j, 0]) * ab[0] + (z - prof[j, 1]) * ab[1]) / (ab @ ab), 0.0, 1.0)
+            d2 = (rho - prof[j, 0] - t * ab[0]) ** 2 + (z - prof[j, 1] - t * ab[1]) ** 2
+            better = d2 < best
+            best = np.where(better, d2, best)
+            seg = np.where(better, j, seg)
+            tb = np.where(better, t, tb)
+        return seg, tb, np.sqrt(best)
 
     # ---- inference (standalone, batched) -------------------------------------
     def predict(self, rho, z):
         """E_rho, E_z at points (numpy), through the library's kernels."""
         torch = _torch()
-        x, r = self.features(np.asarray(rho, dtype=np.float64), np.asarray(z, dtype=np.float64))
+        rho = np.asarray(rho, dtype=np.float64)
+        z = np.asarray(z, dtype=np.float64)
+        seg, t, d = self.closest(rho, z)
+        x = self.features(seg, t, d)
         n = len(x)
         npad = ((n + 127) // 128) * 128
         xb = torch.zeros((npad, 2), dtype=torch.float32, device=self.device)
         xb[:n] = torch.as_tensor(x, device=self.device)
         y = forward(self, xb)[:n].cpu().numpy().astype(np.float64)
-        s = self.scale(r)
-        return y[:, 0] * s, y[:, 1] * s
+        sc = self.scale(seg, t, d)
+        nrm, unit = self.frame(seg)
+        en, et = y[:, 0] * sc, y[:, 1] * sc
+        return en * nrm[:, 0] + et * unit[:, 0], en * nrm[:, 1] + et * unit[:, 1]
 
     def state(self):
-        return dict(params=self.p.cpu().numpy(), zc=self.zc, r0=self.r0, lmin=self.lmin, lmax=self.lmax,
+        return dict(params=self.p.cpu().numpy(), profile=self.profile, sigma=self.sigma, s_end=self.s_end,
                     scale_table=self.scale_table)
+
+    @classmethod
+    def from_state(cls, st, device="cuda"):
+        torch = _torch()
+        m = cls(st["profile"], st["sigma"], float(st["s_end"]), st["scale_table"], device=device)
+        m.p = torch.as_tensor(np.asarray(st["params"], dtype=np.float32), device=m.device)
+        m.p16 = m.p.to(torch.bfloat16)
+        m.pr = m.p16.float()
+        return m
 
     def params_dict(self):
         return {name: self.view(self.p, name).cpu().numpy() for name, _ in PARAM_SHAPES}
@@ -198,18 +255,23 @@ def adam_step(model, work, m, vv, lr, step, beta1=0.9, beta2=0.999, eps=1e-8):
            "adam")
 
 
-def sample_points(geometry, n, rng, d_min=1e-9, d_max=1e-3):
-    """Training points around the z >= 0 part of a BEM profile: a uniform
-    point on a random segment, offset along the outward normal by a
-    log-uniform distance, kept if z >= 0, outside the conductor and below
-    z_handoff.  Returns rho, z (float64)."""
+def sample_points(geometry, n, rng, d_min=1e-9, d_max=1e-3, apex_weight=0.5):
+    """Training points around the z >= 0 part of a BEM profile: a point on a
+    segment (half of them uniform in arclength, half uniform over segment
+    index, which favours the finely meshed apex), offset along the outward
+    normal by a log-uniform distance; kept if z >= 0, outside the conductor,
+    below z_handoff.  Returns rho, z, seg, t, d."""
     prof = geometry.profile
-    up = np.nonzero((prof[:-1, 1] >= 0) | (prof[1:, 1] >= 0))[0]
-    out_r, out_z = [], []
+    up = np.nonzero((prof[:-1, 1] >= 0) & (prof[1:, 1] >= 0))[0]
+    lens = np.linalg.norm(prof[up + 1] - prof[up], axis=-1)
+    cdf = np.cumsum(lens) / lens.sum()
+    out = [[] for _ in range(5)]
     got = 0
     while got < n:
         m = 2 * (n - got) + 1024
-        s = up[rng.integers(0, len(up), m)]
+        by_len = rng.uniform(0, 1, m) >= apex_weight
+        pick = np.where(by_len, np.searchsorted(cdf, rng.uniform(0, 1, m)), rng.integers(0, len(up), m))
+        s = up[np.minimum(pick, len(up) - 1)]
         t = rng.uniform(0, 1, m)
         p = prof[s] + t[:, None] * (prof[s + 1] - prof[s])
         tan = prof[s + 1] - prof[s]
@@ -217,26 +279,15 @@ def sample_points(geometry, n, rng, d_min=1e-9, d_max=1e-3):
         nrm /= np.linalg.norm(nrm, axis=-1, keepdims=True)
         d = np.exp(rng.uniform(np.log(d_min), np.log(d_max), m))
         q = p + d[:, None] * nrm
-        rho, z = np.abs(q[:, 0]), q[:, 1]
-        ok = (z >= 0) & (z < geometry.z_handoff)
+        rho, z = q[:, 0], q[:, 1]
+        ok = (z >= 0) & (z < geometry.z_handoff) & (rho >= 0)
         if geometry.kind == _lib.GEOM_POST_BEM:
             rk = geometry.R
             ok &= ~(((rho <= rk) & (z <= geometry.L)) | (rho * rho + (z - geometry.L) ** 2 <= rk * rk))
-        out_r.append(rho[ok])
-        out_z.append(z[ok])
+        for lst, arr in zip(out, (rho, z, s, t, d)):
+            lst.append(arr[ok])
         got += int(ok.sum())
-    return np.concatenate(out_r)[:n], np.concatenate(out_z)[:n]
-
-
-def feature_frame(geometry):
-    """Centre, length scale and log-radius range of the input features."""
-    if geometry.kind == _lib.GEOM_POST_BEM:
-        zc, r0 = geometry.L, geometry.R
-    elif geometry.kind == _lib.GEOM_TIP_BEM:
-        zc, r0 = 0.0, geometry.R
-    else:
-        zc, r0 = 0.0, max(geometry.R, getattr(geometry, "H", geometry.R))
-    return zc, r0, math.log(0.5), math.log(2.0 * geometry.z_handoff / r0)
+    return tuple(np.concatenate(lst)[:n] for lst in out)
 
 
 def label(geometry, rho, z, chunk=1 << 18):
@@ -253,33 +304,40 @@ def label(geometry, rho, z, chunk=1 << 18):
 
 def train(geometry, n_points=2_000_000, steps=20_000, batch=8192, lr=1e-3, seed=4, device="cuda", log_every=0,
           data=None):
-    """Train the surrogate for a BEM geometry with the library's kernels."""
+    """Train the surrogate for a BEM geometry with the library's kernels.
+    data = (rho, z, seg, t, d, E) skips sampling and labelling."""
     torch = _torch()
     rng = np.random.default_rng(seed)
     if data is None:
-        rho, z = sample_points(geometry, n_points, rng)
+        rho, z, seg, t, d = sample_points(geometry, n_points, rng)
         E = label(geometry, rho, z)
     else:
-        rho, z, E = data
-    zc, r0, lmin, lmax = feature_frame(geometry)
-    # per-log-radius RMS scale of the labels
-    dz = z - zc
-    r = np.sqrt(rho * rho + dz * dz)
-    pos = (np.log(r / r0) - lmin) / (lmax - lmin) * (N_SCALE_BINS - 1)
+        rho, z, seg, t, d, E = data
+    prof = geometry.profile
+    up = (prof[:-1, 1] >= 0) & (prof[1:, 1] >= 0)
+    s_end = float(np.linalg.norm(prof[1:] - prof[:-1], axis=-1)[up].sum())
+    model = FieldSurrogate(prof, geometry.sigma, s_end, np.ones(N_SCALE_BINS), device=device, seed=seed)
+    nrm, unit = model.frame(seg)
+    en = E[:, 0] * nrm[:, 0] + E[:, 1] * nrm[:, 1]
+    et = E[:, 0] * unit[:, 0] + E[:, 1] * unit[:, 1]
+    sig = model.scale(seg, t, d)  # |sigma| part only (table is still ones)
+    ld = np.log(np.clip(d, model.D_MIN, model.D_MAX))
+    pos = (ld - math.log(model.D_MIN)) / (math.log(model.D_MAX) - math.log(model.D_MIN)) * (N_SCALE_BINS - 1)
     b = np.clip(np.rint(pos).astype(int), 0, N_SCALE_BINS - 1)
-    mag2 = np.sum(E * E, -1)
+    mag2 = (en * en + et * et) / (sig * sig)
     table = np.ones(N_SCALE_BINS)
+    filled = np.zeros(N_SCALE_BINS, dtype=bool)
     for k in range(N_SCALE_BINS):
         sel = b == k
         if sel.any():
             table[k] = math.sqrt(mag2[sel].mean())
-    filled = table != 1.0
-    if filled.any():
-        idx = np.arange(N_SCALE_BINS)
-        table = np.exp(np.interp(idx, idx[filled], np.log(table[filled])))
-    model = FieldSurrogate(zc, r0, lmin, lmax, table, device=device, seed=seed)
-    x, _ = model.features(rho, z)
-    y = (E / model.scale(r)[:, None]).astype(np.float32)
+            filled[k] = True
+    idx = np.arange(N_SCALE_BINS)
+    table = np.exp(np.interp(idx, idx[filled], np.log(table[filled])))
+    model.scale_table = table
+    x = model.features(seg, t, d)
+    sc = model.scale(seg, t, d)
+    y = np.stack([en / sc, et / sc], -1).astype(np.float32)
     n = (len(x) // batch) * batch
     X = torch.as_tensor(x[:n], device=model.device)
     Y = torch.as_tensor(y[:n], device=model.device)
@@ -307,5 +365,4 @@ def train(geometry, n_points=2_000_000, steps=20_000, batch=8192, lr=1e-3, seed=
         if log_every and (step % log_every == 0 or step == 1):
             losses.append((step, float(work.loss.item())))
     model.train_log = losses
-    model.train_data = (rho, z, E)
     return model

@@ -51,6 +51,8 @@ extern "C" {
 /* arithmetic forms */
 #define SPT_FORM_FP64 0      /* plain: float64 throughout */
 #define SPT_FORM_MIXED 1     /* pair and BEM panel sums in float32 with Kahan compensation */
+#define SPT_FORM_SURROGATE 2 /* mixed, with the BEM field of points outside a near-surface band
+                                taken from the learned MLP surrogate (tensor cores) */
 
 /* per-group status (SptState.status) */
 #define SPT_GROUP_NEW 0      /* not started: t, h are initialised on first touch */
@@ -164,6 +166,24 @@ typedef struct {
     const double* output_times;
     double* output_rec;
     uint8_t* output_flag;
+    /* learned form (SPT_FORM_SURROGATE, BEM geometries): MLP with inputs
+     * (log distance d to the profile, arclength position of the closest
+     * profile point) and outputs (E_normal, E_tangent) / (|sigma| + floor) /
+     * g(d).  sur_w: FP32 (BF16-rounded) parameters W1[128x2] b1 W2[128x128]
+     * b2 W3 b3 W4 b4 W5[2x128] b5, flat; sur_w16: the same in BF16 (the
+     * tensor-core layers read W2..W4 from it); sur_s_start[n_seg]: arclength
+     * at each segment start; sur_log_scale[64]: ln g on a uniform grid of
+     * ln d over [sur_d_min, sur_d_max].  Points closer than sur_band to the
+     * profile use the exact BEM sum, and so does a hashed sur_spot fraction
+     * of the others, whose surrogate error is recorded in sur_stats
+     * [surrogate points, exact points, spot checks, max relative error
+     * (float bits)]. */
+    const float* sur_w;
+    const void* sur_w16;
+    const double* sur_s_start;
+    const double* sur_log_scale;
+    double sur_s_end, sur_sig_floor, sur_band, sur_spot, sur_d_min, sur_d_max;
+    unsigned long long* sur_stats;
 } SptTraceParams;
 
 /* Scratch bytes spt_trace needs for this state/geometry (work-queue

@@ -15,6 +15,11 @@ from bem_b200 import _lib, surrogate as sg  # noqa: E402
 from oracle import mlp as omlp  # noqa: E402
 
 
+def _toy_model(seed):
+    prof = np.array([[0.0, 1.0], [1.0, 0.0]])
+    return sg.FieldSurrogate(prof, np.ones(2), 1.0, np.ones(sg.N_SCALE_BINS), seed=seed)
+
+
 def _mat(g, shape):
     return (torch.randn(shape, generator=g, device="cuda") * 0.5).to(torch.bfloat16)
 
@@ -58,7 +63,7 @@ def test_gemm_split_k_and_epilogues():
 
 
 def test_training_gradients_match_oracle():
-    model = sg.FieldSurrogate(0.0, 1.0, -1.0, 1.0, np.ones(sg.N_SCALE_BINS), seed=3)
+    model = _toy_model(3)
     rng = np.random.default_rng(0)
     n = 256
     x = rng.uniform(-1, 1, (n, 2)).astype(np.float32)
@@ -82,7 +87,7 @@ def test_training_gradients_match_oracle():
 
 def test_short_training_lowers_loss():
     """Fit a smooth 2-D field for 300 steps: the loss must drop by 10x."""
-    model = sg.FieldSurrogate(0.0, 1.0, -1.0, 1.0, np.ones(sg.N_SCALE_BINS), seed=5)
+    model = _toy_model(5)
     rng = np.random.default_rng(1)
     n = 1024
     x = rng.uniform(-1, 1, (n * 16, 2)).astype(np.float32)
