@@ -86,6 +86,8 @@ SIGNATURES = {
     "spt_accel": (ctypes.c_int, [ctypes.POINTER(SptAccelArgs), ctypes.POINTER(SptGeometry),
                                  ctypes.POINTER(SptBem), _p]),
     "spt_bem_field": (ctypes.c_int, [_p, _p, _p, _i64, ctypes.POINTER(SptBem), _i32, _p, _p, _p, _p]),
+    "spt_surrogate_field": (ctypes.c_int, [_p, _p, _p, _i64, ctypes.POINTER(SptBem), ctypes.POINTER(SptTraceParams),
+                                           _p, _p, _p, _p]),
     "spt_ring_field": (ctypes.c_int, [_p, _p, _p, _i64, _i32, _p, _p, _p]),
     "spt_ellip_ke": (ctypes.c_int, [_p, _i64, _i32, _p, _p, _p]),
     "spt_bem_assemble": (ctypes.c_int, [_p, _p, _i32, _d, _i32, _p, _p, _p, _p]),

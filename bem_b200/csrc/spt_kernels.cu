@@ -33,6 +33,7 @@
 
 #include "../../include/spt_b200.h"
 #include "spt_math.cuh"
+#include "spt_umma.cuh"
 
 namespace spt {
 
@@ -187,6 +188,7 @@ struct Layout {
     int fld;                  // 3E field
     int img;                  // 4E sphere images
     int bpt;                  // 8E per BEM list entry: x y z rho_e z_e near_r near_z (+1 pad)
+    int sur;                  // surrogate region: act (4096), wt (4096), sout 2E, sseg E, st E, sd E, feat 128; -1 if none
     int tiles;                // 2 * 3 * tile_cap
     int tile_cap;             // nodes per TMA tile row
     int red;                  // kWarps * 2 * kRound
@@ -197,7 +199,7 @@ struct Layout {
     bool big;                 // slopes/y0/nw in global memory
 };
 
-__host__ __device__ inline Layout make_layout(int E, bool want_tiles) {
+__host__ __device__ inline Layout make_layout(int E, bool want_tiles, bool want_sur = false) {
     Layout L;
     const bool big = E > kSmallGroup;
     int o = 0;
@@ -219,6 +221,12 @@ __host__ __device__ inline Layout make_layout(int E, bool want_tiles) {
     L.fld = o; o += 3 * E;
     L.img = o; o += 4 * E;
     L.bpt = o; o += 8 * E;
+    if (want_sur) {
+        o = (o + 127) & ~127;  // 1 KiB alignment for the tensor-core operand tiles
+        L.sur = o; o += 8192 + 5 * E + 128;
+    } else {
+        L.sur = -1;
+    }
     o = (o + 1) & ~1;  // 16-byte alignment for the TMA tiles
     const int base = o;
     const int n_ints = 2 * E + kRound * 256 / 4 + 4;  // live, list, near flags (bytes) packed in ints
@@ -256,14 +264,26 @@ struct Ctx {
     int* list;
     unsigned char* nflag;
     uint64_t* bars;
-    uint32_t phase[2];          // parity of the next phase to wait for on bars[0], bars[1] (identical in every thread)
+    uint32_t phase[3];          // parity of the next phase to wait for on bars[0..2] (identical in every thread)
+    // learned form
+    uint8_t *act, *wt;          // BF16 operand tiles (activations, weights), canonical K-major, 32 KiB each
+    double *sout, *st, *sd;     // surrogate E (rho, z) per record; closest-point parameter and distance
+    int* sseg;                  // closest segment per record
+    float* feat;                // features of the current 128-row chunk
+    const float* sw;            // FP32 (BF16-rounded) parameters
+    const __nv_bfloat16* sw16;  // BF16 parameters
+    const double *s_start, *log_scale;
+    double s_end, sig_floor, band, spot, dmin, dmax;
+    unsigned long long* sstats;
+    uint32_t tmem;
+    uint32_t key;               // hash key of the current stage evaluation (spot checks)
     unsigned long long cnt[8];  // per-thread counter partials (thread 0 flushes)
 };
 
-__device__ inline void bind(Ctx& c, double* smem, int E, double* slot) {
+__device__ inline void bind(Ctx& c, double* smem, int E, double* slot, bool sur = false) {
     c.base = smem;
     c.E = E;
-    c.L = make_layout(E, true);
+    c.L = make_layout(E, true, sur);
     const Layout& L = c.L;
     if (!L.big) {
         c.y0 = smem + L.y0;
@@ -293,6 +313,16 @@ __device__ inline void bind(Ctx& c, double* smem, int E, double* slot) {
     c.nflag = reinterpret_cast<unsigned char*>(ib + L.flags_off);
     c.bars = reinterpret_cast<uint64_t*>(smem + L.total_doubles + 1);
     for (int k = 0; k < 8; ++k) c.cnt[k] = 0;
+    if (L.sur >= 0) {
+        double* r = smem + L.sur;
+        c.act = reinterpret_cast<uint8_t*>(r);
+        c.wt = reinterpret_cast<uint8_t*>(r + 4096);
+        c.sout = r + 8192;
+        c.st = c.sout + 2 * E;
+        c.sd = c.st + E;
+        c.sseg = reinterpret_cast<int*>(c.sd + E);
+        c.feat = reinterpret_cast<float*>(c.sd + 2 * E);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -476,17 +506,18 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
 }
 
 // ---------------------------------------------------------------------------
-// BEM field of the n points listed in c.bpt (x, y, z at slots 0..2 of each
-// 8-double record).  Writes the perturbation field into c.fld[3*list[k]..]
-// when `scatter`, else into bpt record slots 5..7 (ex, ey, ez).
-// Must be called by all threads of the CTA.
+// BEM field of a list of points, in phases.  Records live in c.bpt (8 doubles
+// each: x, y, z, rho_e, z_e, then results); every phase is called by all
+// threads of the CTA.
 
-__device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
+// A: closest segment and on-surface offset of records [0, n).  With `frame`,
+// also the closest segment, its parameter t and the distance, for the
+// surrogate's inputs.
+__device__ void bem_closest(Ctx& c, int n, bool frame) {
     const SptBem& b = c.bem;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double* P = c.bpt;  // record k: [0]x [1]y [2]z [3]rho_e [4]z_e [5]ax [6]ay [7]near_r ; near_z in fld tmp
     const int nseg = b.n_seg;
-    const int nps = b.nodes_per_seg;
 
     // A: closest point + on-surface offset (one warp per point)
     for (int k = warp; k < n; k += kWarps) {
@@ -513,10 +544,28 @@ __device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
             if (rho == 0.0) re = 0.0;
             P[8 * k + 3] = re;
             P[8 * k + 4] = __dadd_rn(z, __dmul_rn(off, segf(b, 8, bs)));
+            if (frame) {
+                const double p0x = segf(b, 0, bs), p0y = segf(b, 1, bs), ax = segf(b, 2, bs), ay = segf(b, 3, bs);
+                double tt = ((rho - p0x) * ax + (z - p0y) * ay) / (ax * ax + ay * ay);
+                c.sseg[k] = bs;
+                c.st[k] = fmin(fmax(tt, 0.0), 1.0);
+                c.sd[k] = sqrt(best);
+            }
         }
     }
     __syncthreads();
+}
 
+
+// B + C: exact BEM field (E_rho, E_z into record slots 5, 6) of records [0, n)
+// whose slots 3, 4 hold the evaluation point.
+__device__ void bem_sums(Ctx& c, int n, int* status_flag) {
+    const SptBem& b = c.bem;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* P = c.bpt;
+    const int nseg = b.n_seg;
+    const int nps = b.nodes_per_seg;
+    if (n <= 0) return;
     // B: near-segment sinh quadrature (one warp per point)
     unsigned long long n_near = 0, n_ring_near = 0;
     for (int k = warp; k < n; k += kWarps) {
@@ -575,7 +624,7 @@ __device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
     bool ok = true;
     for (int r0 = 0; r0 < n; r0 += kRound) {
         const int np_ = min(kRound, n - r0);
-        if (c.form == SPT_FORM_MIXED) {
+        if (c.form != SPT_FORM_FP64) {  // mixed, and the exact sums of the learned form
             if (np_ == 1)
                 far_round<1, 8, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
             else if (np_ == 2)
@@ -597,7 +646,12 @@ __device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
     }
     if (!ok && tid == 0) *status_flag = SPT_GROUP_TIMEOUT;
     c.cnt[SPT_CNT_RING_FAR] += far_evals;
-    // D: rotate E_rho into (x, y)
+}
+
+// D: rotate E_rho of records [0, n) into (x, y) (record slots 5, 6, 7 = ex, ey, ez)
+__device__ void bem_rotate(Ctx& c, int n, bool scatter) {
+    const int tid = threadIdx.x;
+    double* P = c.bpt;
     for (int k = tid; k < n; k += kThreads) {
         const double x = P[8 * k + 0], y = P[8 * k + 1];
         const double rho = hypot(x, y);
@@ -619,6 +673,243 @@ __device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
         }
     }
     __syncthreads();
+}
+
+
+// ---------------------------------------------------------------------------
+// learned form: the MLP surrogate evaluated on the tensor cores inside the
+// stage (parameter offsets in the flat parameter array)
+constexpr int kOW1 = 0, kOB1 = 256, kOW2 = 384, kOB2 = 16768, kOW3 = 16896, kOB3 = 33280, kOW4 = 33408, kOB4 = 49792,
+              kOW5 = 49920, kOB5 = 50176;
+
+// Surrogate field (E_rho, E_z) of records [0, n) into c.sout, from the
+// closest-point frame bem_closest(c, n, true) left in sseg/st/sd.  Rows are
+// processed 128 at a time: features and the first layer on the CUDA cores
+// into a BF16 activation tile, three 128 x 128 layers as tcgen05.mma (K = 16
+// steps) into the CTA's TMEM accumulator with the weights streamed into a
+// BF16 tile, bias + SiLU applied while reading TMEM back, the last layer on
+// the CUDA cores, then rescaling and rotation from the (normal, tangent)
+// frame of the closest segment.
+__device__ void mlp_points(Ctx& c, int n, int* status_flag) {
+    const SptBem& b = c.bem;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const float* W = c.sw;
+    const double lmin = log(c.dmin), lspan = log(c.dmax) - lmin;
+    for (int cs = 0; cs < n; cs += 128) {
+        const int m = min(128, n - cs);
+        if (tid < 128) {
+            float u1 = 0.f, u2 = 0.f;
+            if (tid < m) {
+                const int k = cs + tid;
+                const int sg = c.sseg[k];
+                const double sarc = (c.s_start[sg] + c.st[k] * segf(b, 4, sg)) / c.s_end;
+                const double ld = log(fmin(fmax(c.sd[k], c.dmin), c.dmax));
+                u1 = (float)(2.0 * (ld - lmin) / lspan - 1.0);
+                u2 = (float)(2.0 * sarc - 1.0);
+            }
+            c.feat[2 * tid] = u1;
+            c.feat[2 * tid + 1] = u2;
+        }
+        __syncthreads();
+        for (int idx = tid; idx < 128 * 128; idx += kThreads) {
+            const int r = idx >> 7, j = idx & 127;
+            float h = 0.f;
+            if (r < m) {
+                const float v = fmaf(W[kOW1 + 2 * j], c.feat[2 * r], fmaf(W[kOW1 + 2 * j + 1], c.feat[2 * r + 1], W[kOB1 + j]));
+                h = spt_umma::silu(v);
+            }
+            *reinterpret_cast<__nv_bfloat16*>(c.act + spt_umma::kmajor128(r, j)) = __float2bfloat16_rn(h);
+        }
+        for (int l = 0; l < 3; ++l) {
+            const int ow = l == 0 ? kOW2 : (l == 1 ? kOW3 : kOW4);
+            const int ob = l == 0 ? kOB2 : (l == 1 ? kOB3 : kOB4);
+            // weights as the B operand: element (n = out, k = in) at W16[ow + n*128 + k], K-major
+            for (int v = tid; v < 2048; v += kThreads) {
+                const int nrow = v >> 4, kg = v & 15;
+                const uint4 val = *reinterpret_cast<const uint4*>(c.sw16 + ow + nrow * 128 + kg * 8);
+                *reinterpret_cast<uint4*>(c.wt + ((nrow >> 3) * 16 + kg) * 128 + (nrow & 7) * 16) = val;
+            }
+            spt_umma::fence_proxy();
+            __syncthreads();
+            if (tid == 0) {
+                spt_umma::fence_after();
+                const uint32_t idesc = spt_umma::idesc_bf16_128(0, 0);
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk)
+                    spt_umma::mma(c.tmem, spt_umma::desc(c.act + kk * 256, 128, 2048),
+                                  spt_umma::desc(c.wt + kk * 256, 128, 2048), idesc, kk > 0 ? 1u : 0u);
+                spt_umma::commit(&c.bars[2]);
+            }
+            const bool ok = mbar_wait(&c.bars[2], c.phase[2]);
+            c.phase[2] ^= 1u;
+            if (!ok && tid == 0) *status_flag = SPT_GROUP_TIMEOUT;
+            spt_umma::fence_after();
+            // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows), columns 64 (w / 4) .. +63
+            const int row = 32 * (warp & 3) + lane;
+            const int cb = 64 * (warp >> 2);
+#pragma unroll
+            for (int c0 = 0; c0 < 64; c0 += 16) {
+                float v[16];
+                spt_umma::ld16(c.tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(cb + c0), v);
+#pragma unroll
+                for (int i = 0; i < 16; ++i) {
+                    const int col = cb + c0 + i;
+                    const float h = spt_umma::silu(v[i] + W[ob + col]);
+                    *reinterpret_cast<__nv_bfloat16*>(c.act + spt_umma::kmajor128(row, col)) = __float2bfloat16_rn(h);
+                }
+            }
+            spt_umma::fence_before();
+            spt_umma::fence_proxy();
+            __syncthreads();
+        }
+        // last layer, rescaling and rotation: one warp per row
+        for (int r = warp; r < m; r += kWarps) {
+            float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int j = lane + 32 * q;
+                const float h = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(c.act + spt_umma::kmajor128(r, j)));
+                a0 = fmaf(W[kOW5 + j], h, a0);
+                a1 = fmaf(W[kOW5 + 128 + j], h, a1);
+            }
+            a0 = warp_sum(a0);
+            a1 = warp_sum(a1);
+            if (lane == 0) {
+                const int k = cs + r;
+                const int sg = c.sseg[k];
+                const double t = c.st[k];
+                const double sig = fabs(segf(b, 9, sg) + t * (segf(b, 10, sg) - segf(b, 9, sg))) + c.sig_floor;
+                const double pos = (log(fmin(fmax(c.sd[k], c.dmin), c.dmax)) - lmin) / lspan * 63.0;
+                const int i0 = min(62, max(0, (int)floor(pos)));
+                const double fr = fmin(fmax(pos - i0, 0.0), 1.0);
+                const double g = exp(c.log_scale[i0] + fr * (c.log_scale[i0 + 1] - c.log_scale[i0]));
+                const double en = ((double)a0 + (double)W[kOB5]) * sig * g;
+                const double et = ((double)a1 + (double)W[kOB5 + 1]) * sig * g;
+                c.sout[2 * k] = en * segf(b, 7, sg) + et * segf(b, 5, sg);
+                c.sout[2 * k + 1] = en * segf(b, 8, sg) + et * segf(b, 6, sg);
+            }
+        }
+        __syncthreads();
+    }
+}
+
+__device__ __forceinline__ bool spot_pick(uint32_t key, int particle, double frac) {
+    uint32_t h = key * 0x9E3779B1u ^ (uint32_t)particle * 0x85EBCA77u;
+    h ^= h >> 15;
+    h *= 0x2C1B3C6Du;
+    h ^= h >> 12;
+    return (double)(h & 0xFFFFu) < frac * 65536.0;
+}
+
+// BEM field of the listed points in the learned form: the surrogate for
+// every point, the exact sum for points within the band and for the spot
+// checks (stable partition: exact records first), surrogate error of the
+// spot checks recorded, then the rotation of phase D.
+__device__ void surrogate_points(Ctx& c, int n, int* status_flag) {
+    const int tid = threadIdx.x;
+    double* P = c.bpt;
+    __shared__ int s_cnt[kWarps + 1];
+    __shared__ int s_tot[2];
+    bem_closest(c, n, true);
+    mlp_points(c, n, status_flag);
+    // stable partition of records [0, n): exact (band or spot) first.  The
+    // destination of every record is found first (kept in sseg, which the
+    // MLP no longer needs), then the records move through the act/wt scratch
+    // (8 doubles each: slots 0-4 of the record, the surrogate E_rho, E_z, and
+    // the list entry, negated minus one when the point lies in the band).
+    if (tid == 0) s_tot[0] = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += kThreads) {
+        const int k = base + tid;
+        const bool ex = k < n && (c.sd[k] < c.band || spot_pick(c.key, c.list[k], c.spot));
+        const unsigned bal = __ballot_sync(0xffffffffu, ex);
+        if ((tid & 31) == 0 && bal) atomicAdd(&s_tot[0], __popc(bal));
+    }
+    __syncthreads();
+    const int ne = s_tot[0];
+    int run_ex = 0, run_su = 0;
+    for (int base = 0; base < n; base += kThreads) {
+        const int k = base + tid;
+        const bool valid = k < n;
+        const bool band = valid && c.sd[k] < c.band;
+        const bool ex = valid && (band || spot_pick(c.key, c.list[k], c.spot));
+        const unsigned be = __ballot_sync(0xffffffffu, ex);
+        if ((tid & 31) == 0) s_cnt[tid >> 5] = __popc(be);
+        __syncthreads();
+        int pre_e = 0, tot_e = 0;
+        for (int w = 0; w < kWarps; ++w) {
+            if (w < (tid >> 5)) pre_e += s_cnt[w];
+            tot_e += s_cnt[w];
+        }
+        const int chunk = min(kThreads, n - base);
+        const int before = min((tid >> 5) * 32, chunk);  // records of this chunk before this warp
+        const unsigned lt = (1u << (tid & 31)) - 1u;
+        if (valid) {
+            const int lane_e = __popc(be & lt);
+            const int dst = ex ? run_ex + pre_e + lane_e : ne + run_su + (before - pre_e) + ((tid & 31) - lane_e);
+            c.sseg[k] = 2 * dst + (band ? 1 : 0);
+        }
+        run_ex += tot_e;
+        run_su += chunk - tot_e;
+        __syncthreads();
+    }
+    double* tmp = reinterpret_cast<double*>(c.act);  // act + wt: 8192 doubles >= 8 n
+    for (int k = tid; k < n; k += kThreads) {
+        const int code = c.sseg[k];
+        const int d = code >> 1;
+        for (int f = 0; f < 5; ++f) tmp[8 * d + f] = P[8 * k + f];
+        tmp[8 * d + 5] = c.sout[2 * k];
+        tmp[8 * d + 6] = c.sout[2 * k + 1];
+        tmp[8 * d + 7] = (code & 1) ? -(double)c.list[k] - 1.0 : (double)c.list[k];
+    }
+    __syncthreads();
+    for (int k = tid; k < n; k += kThreads) {
+        for (int f = 0; f < 5; ++f) P[8 * k + f] = tmp[8 * k + f];
+        c.sout[2 * k] = tmp[8 * k + 5];
+        c.sout[2 * k + 1] = tmp[8 * k + 6];
+        const double v = tmp[8 * k + 7];
+        c.list[k] = v < 0.0 ? (int)(-v - 1.0) : (int)v;
+        c.fld[3 * k] = v < 0.0 ? 1.0 : 0.0;  // band flag, kept where the sums do not write
+    }
+    __syncthreads();
+    bem_sums(c, ne, status_flag);
+    unsigned long long n_spot = 0, n_band = 0;
+    for (int k = tid; k < n; k += kThreads) {
+        if (k >= ne) {
+            P[8 * k + 5] = c.sout[2 * k];
+            P[8 * k + 6] = c.sout[2 * k + 1];
+        } else if (c.fld[3 * k] == 0.0) {  // a spot check: exact and surrogate both known
+            // error relative to the whole external field there (uniform + perturbation)
+            const double er = P[8 * k + 5], ez = P[8 * k + 6];
+            const double dr = c.sout[2 * k] - er, dz = c.sout[2 * k + 1] - ez;
+            const double tz = ez + c.g.E_gun;
+            const float rel = (float)(sqrt(dr * dr + dz * dz) / fmax(sqrt(er * er + tz * tz), 1e-300));
+            if (c.sstats) atomicMax(reinterpret_cast<unsigned int*>(c.sstats) + 6, __float_as_uint(rel));
+            ++n_spot;
+        } else {
+            ++n_band;
+        }
+    }
+    if (c.sstats) {
+        const unsigned long long nsur = (unsigned long long)(n - ne);
+        if (tid == 0 && nsur) atomicAdd(c.sstats + 0, nsur);
+        n_band = warp_sum(n_band);
+        n_spot = warp_sum(n_spot);
+        if ((tid & 31) == 0) {
+            if (n_band) atomicAdd(c.sstats + 1, n_band);
+            if (n_spot) atomicAdd(c.sstats + 2, n_spot);
+        }
+    }
+    __syncthreads();
+    bem_rotate(c, n, false);
+}
+
+// BEM field of the n points listed in c.bpt (x, y, z at slots 0..2 of each
+// 8-double record): the reference's evaluation, phases A-D.
+__device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
+    bem_closest(c, n, false);
+    bem_sums(c, n, status_flag);
+    bem_rotate(c, n, scatter);
 }
 
 // Softened pair sum over the live sources of the group (forces.py:16-29):
@@ -709,7 +1000,12 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
             n_list += s_wcount[kWarps];
             __syncthreads();
         }
-        if (n_list > 0) bem_points(c, n_list, false, status_flag);
+        if (n_list > 0) {
+            if (c.form == SPT_FORM_SURROGATE)
+                surrogate_points(c, n_list, status_flag);
+            else
+                bem_points(c, n_list, false, status_flag);
+        }
         // scatter: fld[i] = blended field
         for (int i = tid; i < E; i += kThreads) { c.fld[3 * i + 0] = 0.0; c.fld[3 * i + 1] = 0.0; c.fld[3 * i + 2] = 0.0; }
         __syncthreads();
@@ -769,7 +1065,7 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
                 ez = w * nz + (1.0 - w) * fz;
             }
             const double qk = c.kc * c.q[i];
-            const bool mix = c.form == SPT_FORM_MIXED;
+            const bool mix = c.form != SPT_FORM_FP64;
             double fcx = 0.0, fcy = 0.0, fcz = 0.0;
             if (E > 1) {
                 auto real = [&](int j, double& x, double& y, double& z, double& q) {
@@ -844,9 +1140,11 @@ __device__ inline void flush_counters(Ctx& c, unsigned long long* counters) {
 __device__ inline void init_barriers(Ctx& c) {
     c.phase[0] = 0u;
     c.phase[1] = 0u;
+    c.phase[2] = 0u;
     if (threadIdx.x == 0) {
         mbar_init(&c.bars[0], 1);
         mbar_init(&c.bars[1], 1);
+        mbar_init(&c.bars[2], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -949,6 +1247,33 @@ __device__ __forceinline__ void write_output(const SptTraceParams& prm, long lon
     prm.output_flag[(size_t)k * n_particles + pidx] = 1;
 }
 
+// learned-form parameters into the context, and the CTA's 128 TMEM columns
+// (the 128 x 128 FP32 accumulator) for its whole lifetime; all threads call
+__device__ void bind_surrogate(Ctx& c, const SptTraceParams& prm, uint32_t* s_tmem) {
+    c.sw = prm.sur_w;
+    c.sw16 = static_cast<const __nv_bfloat16*>(prm.sur_w16);
+    c.s_start = prm.sur_s_start;
+    c.log_scale = prm.sur_log_scale;
+    c.s_end = prm.sur_s_end;
+    c.sig_floor = prm.sur_sig_floor;
+    c.band = prm.sur_band;
+    c.spot = prm.sur_spot;
+    c.dmin = prm.sur_d_min;
+    c.dmax = prm.sur_d_max;
+    c.sstats = prm.sur_stats;
+    if ((threadIdx.x >> 5) == 0) spt_umma::alloc(s_tmem, 128);
+    spt_umma::fence_before();
+    __syncthreads();
+    spt_umma::fence_after();
+    c.tmem = *s_tmem;
+}
+
+__device__ void release_surrogate(Ctx& c) {
+    spt_umma::fence_before();
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) spt_umma::dealloc(c.tmem, 128);
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(kThreads, 1)
 trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* work, double* big_slots) {
@@ -966,7 +1291,10 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
     c.soft2 = prm.plummer_radius * prm.plummer_radius;
     c.form = prm.form;
     const int Emax = st.max_group_size;
-    bind(c, smem, Emax, big_slots ? big_slots + (size_t)blockIdx.x * big_slot_doubles(Emax) : nullptr);
+    const bool sur = prm.form == SPT_FORM_SURROGATE;
+    bind(c, smem, Emax, big_slots ? big_slots + (size_t)blockIdx.x * big_slot_doubles(Emax) : nullptr, sur);
+    __shared__ uint32_t s_tmem;
+    if (sur) bind_surrogate(c, prm, &s_tmem);
     init_barriers(c);
 
     for (;;) {
@@ -1078,6 +1406,7 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
                     }
                 }
                 __syncthreads();
+                c.key = (uint32_t)g * 2654435761u ^ (uint32_t)(gs.n_acc + gs.n_rej) * 40503u ^ (uint32_t)s * 97u;
                 stage_accel<KIND>(c, kv[s], &s_flag);
             }
             // 5th-order solution and the endpoint stage (batched_rk45.py:365-370)
@@ -1097,6 +1426,7 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
                 }
             }
             __syncthreads();
+            c.key = (uint32_t)g * 2654435761u ^ (uint32_t)(gs.n_acc + gs.n_rej) * 40503u ^ 6u * 97u;
             stage_accel<KIND>(c, kv[6], &s_flag);
             // embedded error norm (batched_rk45.py:372-393)
             double part = 0.0;
@@ -1194,6 +1524,7 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
         // stop taking groups (the remaining ones stay NEW/RUNNING for the host).
         if (s_flag == SPT_GROUP_TIMEOUT) break;
     }
+    if (sur) release_surrogate(c);
 }
 
 // one stage evaluation per group (spt_accel)
@@ -1265,6 +1596,45 @@ bem_field_kernel(const double* x, const double* y, const double* z, long long n,
         ez[p0 + k] = c.bpt[8 * k + 7];
     }
     flush_counters(c, counters);
+}
+
+// learned-form field at arbitrary points (spt_surrogate_field): 128 points
+// (one MLP tile) per CTA, through the stage kernel's surrogate_points
+constexpr int kSurChunk = 128;
+__global__ void __launch_bounds__(kThreads, 1)
+surrogate_field_kernel(const double* x, const double* y, const double* z, long long n, SptBem bem, SptTraceParams prm,
+                       double* ex, double* ey, double* ez, unsigned long long* counters) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int s_flag;
+    __shared__ uint32_t s_tmem;
+    Ctx c;
+    c.g = SptGeometry{};
+    c.bem = bem;
+    c.form = SPT_FORM_SURROGATE;
+    bind(c, smem, kSurChunk, nullptr, true);
+    bind_surrogate(c, prm, &s_tmem);
+    init_barriers(c);
+    c.key = 0x2545F491u;
+    const long long p0 = (long long)blockIdx.x * kSurChunk;
+    const int np_ = (int)min((long long)kSurChunk, n - p0);
+    for (int k = threadIdx.x; k < np_; k += kThreads) {
+        c.bpt[8 * k + 0] = x[p0 + k];
+        c.bpt[8 * k + 1] = y[p0 + k];
+        c.bpt[8 * k + 2] = z[p0 + k];
+        c.list[k] = (int)(p0 + k);
+    }
+    if (threadIdx.x == 0) s_flag = 0;
+    __syncthreads();
+    surrogate_points(c, np_, &s_flag);
+    // records were reordered (exact ones first): c.list holds each one's point index
+    for (int k = threadIdx.x; k < np_; k += kThreads) {
+        const long long i = c.list[k];
+        ex[i] = c.bpt[8 * k + 5];
+        ey[i] = c.bpt[8 * k + 6];
+        ez[i] = c.bpt[8 * k + 7];
+    }
+    flush_counters(c, counters);
+    release_surrogate(c);
 }
 
 __global__ void ring_kernel(const double* rho, const double* z, const double* a, long long n, int form, double* er,
@@ -1389,6 +1759,22 @@ int check_bem(const SptBem* b) {
 
 bool is_bem(int kind) { return kind == SPT_GEOM_TIP_BEM || kind == SPT_GEOM_WELL_BEM || kind == SPT_GEOM_POST_BEM; }
 
+int check_surrogate_params(const SptTraceParams* p) {
+    if (!p->sur_w || !p->sur_w16 || !p->sur_s_start || !p->sur_log_scale)
+        return fail(SPT_ERR_ARG, "learned form: surrogate parameters missing");
+    if (reinterpret_cast<uintptr_t>(p->sur_w16) & 15) return fail(SPT_ERR_ARG, "sur_w16 must be 16-byte aligned");
+    if (!(p->sur_d_min > 0.0) || !(p->sur_d_max > p->sur_d_min) || !(p->sur_s_end > 0.0))
+        return fail(SPT_ERR_ARG, "learned form: bad feature ranges");
+    return SPT_OK;
+}
+
+// (groups are at most 1024 particles in every form: surrogate_points
+// reorders a stage's points through the 64 KiB MLP operand tiles, 8 doubles each)
+int check_surrogate(const SptTraceParams* p, const SptGeometry* g) {
+    if (!is_bem(g->kind)) return fail(SPT_ERR_ARG, "the learned form needs a BEM geometry");
+    return check_surrogate_params(p);
+}
+
 template <typename K>
 int set_smem(K kernel, size_t bytes) {
     return cuda_check(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes),
@@ -1406,7 +1792,7 @@ int grid_for(int n_groups, int blocks_per_sm_hint) {
 template <int KIND>
 int launch_trace(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b, void* ws,
                  int64_t ws_bytes, cudaStream_t stream) {
-    const spt::Layout L = spt::make_layout(s->max_group_size, true);
+    const spt::Layout L = spt::make_layout(s->max_group_size, true, p->form == SPT_FORM_SURROGATE);
     auto kern = spt::trace_kernel<KIND>;
     int rc = set_smem(kern, L.bytes);
     if (rc) return rc;
@@ -1462,9 +1848,14 @@ int spt_trace(const SptState* s, const SptTraceParams* p, const SptGeometry* g, 
     if (s->max_group_size <= 0 || s->max_group_size > 1024)
         return fail(SPT_ERR_CAPACITY, "max_group_size %d outside [1, 1024]", s->max_group_size);
     if (reinterpret_cast<uintptr_t>(ws) & 255) return fail(SPT_ERR_ARG, "workspace must be 256-byte aligned");
-    if (p->form != SPT_FORM_FP64 && p->form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "unknown form %d", p->form);
+    if (p->form != SPT_FORM_FP64 && p->form != SPT_FORM_MIXED && p->form != SPT_FORM_SURROGATE)
+        return fail(SPT_ERR_ARG, "unknown form %d", p->form);
     if (is_bem(g->kind)) {
         const int rc = check_bem(b);
+        if (rc) return rc;
+    }
+    if (p->form == SPT_FORM_SURROGATE) {
+        const int rc = check_surrogate(p, g);
         if (rc) return rc;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -1483,6 +1874,7 @@ int spt_accel(const SptAccelArgs* a, const SptGeometry* g, const SptBem* b, void
     if (a->n_groups <= 0) return SPT_OK;
     if (a->max_group_size <= 0 || a->max_group_size > spt::kSmallGroup)
         return fail(SPT_ERR_CAPACITY, "spt_accel: group size must be in [1, %d]", spt::kSmallGroup);
+    if (a->form != SPT_FORM_FP64 && a->form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "spt_accel: form %d", a->form);
     if (is_bem(g->kind)) {
         const int rc = check_bem(b);
         if (rc) return rc;
@@ -1524,6 +1916,24 @@ int spt_bem_field(const double* x, const double* y, const double* z, int64_t n, 
     spt::bem_field_kernel<<<(unsigned)blocks, spt::kThreads, L.bytes, static_cast<cudaStream_t>(stream)>>>(
         x, y, z, n, *b, form, ex, ey, ez, nullptr);
     return cuda_check(cudaGetLastError(), "bem_field_kernel launch");
+}
+
+int spt_surrogate_field(const double* x, const double* y, const double* z, int64_t n, const SptBem* b,
+                        const SptTraceParams* sur, double* ex, double* ey, double* ez, void* stream) {
+    if (n <= 0) return SPT_OK;
+    if (!x || !y || !z || !ex || !ey || !ez || !sur) return fail(SPT_ERR_ARG, "null argument");
+    int rc = check_bem(b);
+    if (rc) return rc;
+    rc = check_surrogate_params(sur);
+    if (rc) return rc;
+    const spt::Layout L = spt::make_layout(spt::kSurChunk, true, true);
+    rc = set_smem(spt::surrogate_field_kernel, L.bytes);
+    if (rc) return rc;
+    const long long blocks = (n + spt::kSurChunk - 1) / spt::kSurChunk;
+    if (blocks > 0x7fffffffLL) return fail(SPT_ERR_CAPACITY, "too many points");
+    spt::surrogate_field_kernel<<<(unsigned)blocks, spt::kThreads, L.bytes, static_cast<cudaStream_t>(stream)>>>(
+        x, y, z, n, *b, *sur, ex, ey, ez, nullptr);
+    return cuda_check(cudaGetLastError(), "surrogate_field_kernel launch");
 }
 
 int spt_ring_field(const double* rho, const double* z, const double* a, int64_t n, int32_t form, double* er,
@@ -1597,7 +2007,7 @@ int noalloc_scratch(void** out) {
 template <int KIND>
 int launch_trace_noalloc(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b,
                          unsigned char* scratch, cudaStream_t stream) {
-    const spt::Layout L = spt::make_layout(s->max_group_size, true);
+    const spt::Layout L = spt::make_layout(s->max_group_size, true, p->form == SPT_FORM_SURROGATE);
     auto kern = spt::trace_kernel<KIND>;
     int rc = set_smem(kern, L.bytes);
     if (rc) return rc;
@@ -1632,6 +2042,7 @@ extern "C" int spt_trace_noalloc(const SptState* s, const SptTraceParams* p, con
     if (s->max_group_size <= 0 || s->max_group_size > 1024)
         return fail(SPT_ERR_CAPACITY, "spt_trace_noalloc: max_group_size %d outside [1, 1024]", s->max_group_size);
     if (p->form != SPT_FORM_FP64 && p->form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "unknown form %d", p->form);
+    if (p->form == SPT_FORM_SURROGATE) return fail(SPT_ERR_ARG, "spt_trace_noalloc: the learned form is not offered");
     if (is_bem(g->kind)) {
         const int rc = check_bem(b);
         if (rc) return rc;

@@ -101,13 +101,16 @@ class GroupBatch:
         return torch.stack([self.vx, self.vy, self.vz], dim=-1)
 
 
-FORMS = {"fp64": _lib.FORM_FP64, "mixed": _lib.FORM_MIXED}
+FORMS = {"fp64": _lib.FORM_FP64, "mixed": _lib.FORM_MIXED, "surrogate": _lib.FORM_SURROGATE}
 
 
 class Tracer:
     """Persistent-kernel RK45 tracer for one geometry on one device."""
 
-    def __init__(self, geometry, device="cuda", form="fp64", z_max=None):
+    def __init__(self, geometry, device="cuda", form="fp64", z_max=None, surrogate=None, band=5e-9, spot=0.01):
+        """form: "fp64" (plain), "mixed" (float32 + Kahan sums) or "surrogate"
+        (mixed, with the learned field outside the `band` [m] around the
+        surface, `spot` of the other points checked against the exact sum)."""
         torch = _torch()
         self.geometry = geometry
         self.device = torch.device(device)
@@ -117,6 +120,11 @@ class Tracer:
         self.tables = geometry.bem_tables(self.device) if geometry.is_bem else None
         self._ws = None
         self.counters = torch.zeros(_lib.N_COUNTERS, dtype=torch.int64, device=self.device)
+        self.surrogate = None
+        if self.form == _lib.FORM_SURROGATE:
+            if surrogate is None:
+                raise ValueError("form='surrogate' needs a trained FieldSurrogate")
+            self.surrogate = SurrogateBinding(surrogate, band, spot, self.device)
 
     def params(self, t_max, rtol, atol, plummer_radius, charge_to_mass, max_attempts, log=None,
                safety=0.9, min_factor=0.2, max_factor=10.0, initial_step_fraction=1e-6,
@@ -137,7 +145,12 @@ class Tracer:
         p.counters = self.counters.data_ptr()
         if records is not None:
             records.fill(p)
+        if self.surrogate is not None:
+            self.surrogate.fill(p)
         return p
+
+    def surrogate_stats(self):
+        return self.surrogate.stats()
 
     def workspace(self, state, params):
         torch = _torch()
@@ -334,6 +347,75 @@ def bem_field(tables, points, form="fp64"):
                                         ctypes.byref(tables.struct), FORMS[form] if isinstance(form, str) else form,
                                         out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(),
                                         ctypes.c_void_p(stream.cuda_stream)), "spt_bem_field")
+    return torch.stack(out, dim=-1)
+
+
+class SurrogateBinding:
+    """Device-side parameters of a trained FieldSurrogate for the learned
+    form: the sur_* fields of SptTraceParams, and the statistics buffer
+    (surrogate points, band points, spot checks, max spot error).  The
+    parameters are copied when the binding is made: the FP32 set the stage
+    kernel reads holds the BF16-rounded weights and the FP32 biases, as the
+    standalone network uses them."""
+
+    def __init__(self, model, band=5e-9, spot=0.01, device="cuda"):
+        torch = _torch()
+        d = torch.device(device)
+        self.model = model
+        self.w = model.pr.clone()
+        for name, _ in sg_param_shapes():
+            if name.startswith("b"):
+                model.view(self.w, name).copy_(model.view(model.p, name))
+        self.w16 = model.p16.clone()
+        self.band, self.spot = float(band), float(spot)
+        self.s_start = torch.as_tensor(model.s_start, dtype=torch.float64, device=d)
+        self.log_scale = torch.as_tensor(np.log(model.scale_table), dtype=torch.float64, device=d)
+        self.stats_buf = torch.zeros(4, dtype=torch.int64, device=d)
+        if self.w16.data_ptr() % 16:
+            raise ValueError("surrogate BF16 parameters must be 16-byte aligned")
+
+    def fill(self, p):
+        m = self.model
+        p.sur_w = self.w.data_ptr()
+        p.sur_w16 = self.w16.data_ptr()
+        p.sur_s_start = self.s_start.data_ptr()
+        p.sur_log_scale = self.log_scale.data_ptr()
+        p.sur_s_end, p.sur_sig_floor = float(m.s_end), float(m.sig_floor)
+        p.sur_band, p.sur_spot = self.band, self.spot
+        p.sur_d_min, p.sur_d_max = float(m.D_MIN), float(m.D_MAX)
+        p.sur_stats = self.stats_buf.data_ptr()
+        return p
+
+    def reset(self):
+        self.stats_buf.zero_()
+
+    def stats(self):
+        """(surrogate points, band points, spot checks, max spot error relative
+        to the whole external field at the point)."""
+        v = self.stats_buf.cpu().numpy()
+        err = np.array([v[3] & 0xFFFFFFFF], dtype=np.uint32).view(np.float32)[0]
+        return int(v[0]), int(v[1]), int(v[2]), float(err)
+
+
+def sg_param_shapes():
+    from .surrogate import PARAM_SHAPES
+    return PARAM_SHAPES
+
+
+def surrogate_field(tables, binding, points):
+    """Learned-form perturbation field at points [N, 3] (spt_surrogate_field):
+    the surrogate outside the binding's band, exact inside it and for its
+    spot checks."""
+    torch = _torch()
+    p = _as_dev(points, torch.float64, tables.seg.device).reshape(-1, 3)
+    x, y, z = (p[:, k].contiguous() for k in range(3))
+    out = [torch.empty_like(x) for _ in range(3)]
+    prm = binding.fill(_lib.SptTraceParams())
+    stream = torch.cuda.current_stream(tables.seg.device)
+    _lib.check(_lib.lib().spt_surrogate_field(x.data_ptr(), y.data_ptr(), z.data_ptr(), x.numel(),
+                                              ctypes.byref(tables.struct), ctypes.byref(prm), out[0].data_ptr(),
+                                              out[1].data_ptr(), out[2].data_ptr(),
+                                              ctypes.c_void_p(stream.cuda_stream)), "spt_surrogate_field")
     return torch.stack(out, dim=-1)
 
 

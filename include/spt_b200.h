@@ -19,6 +19,9 @@
  *   spt_accel      the accel(pos, vel, active, group_idx) closure geometry.py:289-299
  *   spt_bem_field  AxisymmetricBEMSolution.field(points)  bem/axisymmetric.py:474-487
  *                  -> evaluate_axisymmetric_field         bem/axisymmetric.py:501-605
+ *   spt_surrogate_field  the learned-form field (no reference counterpart:
+ *                  an MLP stand-in for evaluate_axisymmetric_field, exact
+ *                  within a band around the surface)
  *   spt_ring_field ring_field(rho, z, a)                  bem/axisymmetric.py:235-265
  *   spt_ellip_ke   ellip_ke_complement(p)                 bem/_elliptic.py:28-39
  *   spt_bem_assemble  the collocation matrix of AxisymmetricBEMSolution.solve
@@ -225,6 +228,15 @@ int spt_accel(const SptAccelArgs* args, const SptGeometry* geom, const SptBem* b
  * (x, y, z) -> (ex, ey, ez), all [n] device arrays. */
 int spt_bem_field(const double* x, const double* y, const double* z, int64_t n, const SptBem* bem,
                   int32_t form, double* ex, double* ey, double* ez, void* stream);
+
+/* Learned-form perturbation field at n points: the surrogate MLP (sur_*
+ * fields of `sur`; the other fields are ignored) outside sur_band metres of
+ * the profile, the exact sum of spt_bem_field (mixed form) inside it and for
+ * the sur_spot fraction of points spot-checked, statistics into sur_stats
+ * when it is not NULL.  Same device code as the learned-form stages of
+ * spt_trace. */
+int spt_surrogate_field(const double* x, const double* y, const double* z, int64_t n, const SptBem* bem,
+                        const SptTraceParams* sur, double* ex, double* ey, double* ez, void* stream);
 
 /* Unit-charge ring field (E_rho, E_z) at (rho, z) for ring radius a; [n]. */
 int spt_ring_field(const double* rho, const double* z, const double* a, int64_t n, int32_t form,
