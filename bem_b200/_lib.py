@@ -14,11 +14,15 @@ LIB_PATH = os.path.join(HERE, "libspt_b200.so")
 SPT_OK, SPT_ERR_ARG, SPT_ERR_CUDA, SPT_ERR_CAPACITY = 0, 1, 2, 3
 GEOM_FLAT, GEOM_TIP, GEOM_TIP_BEM, GEOM_WELL_BEM, GEOM_POST_BEM = 0, 1, 2, 3, 4
 FORM_FP64, FORM_MIXED, FORM_SURROGATE = 0, 1, 2
+FAR_REFERENCE, FAR_ADAPTIVE = 0, 1
+FAR_RULES = {"reference": FAR_REFERENCE, "adaptive": FAR_ADAPTIVE}
 GROUP_NEW, GROUP_RUNNING, GROUP_DONE, GROUP_NONFINITE, GROUP_TIMEOUT = 0, 1, 2, 3, 4
 COUNTERS = ("attempts", "accepted", "particle_steps", "stage_evals", "pair_evals", "ring_far", "ring_near",
             "near_pairs")
 N_COUNTERS = len(COUNTERS)
 SEG_FIELDS = 11
+BLOCK_SEGS = 32
+RUN_NODES = 8
 
 _d = ctypes.c_double
 _i32 = ctypes.c_int32
@@ -34,7 +38,10 @@ class SptGeometry(ctypes.Structure):
 
 class SptBem(ctypes.Structure):
     _fields_ = [("n_seg", _i32), ("nodes_per_seg", _i32), ("seg_stride", _i64), ("node_stride", _i64),
-                ("seg", _p), ("node", _p), ("gauss8_x", _d * 8), ("gauss8_w", _d * 8)]
+                ("seg", _p), ("node", _p), ("gauss8_x", _d * 8), ("gauss8_w", _d * 8),
+                ("far_rule", _i32), ("reserved", _i32), ("ratio4", _d), ("ratio2", _d), ("coarse", _p),
+                ("coarse_stride", _i64), ("blk", _p), ("blk_stride", _i64), ("ratio_run", _d), ("run_nodes", _p),
+                ("run_stride", _i64)]
 
 
 class SptState(ctypes.Structure):

@@ -358,6 +358,17 @@ __device__ __forceinline__ bool seg_near(const SptBem& b, int s, double re, doub
     return dist < L;
 }
 
+// Runs of SPT_BLOCK_SEGS consecutive segments (SptBem.blk): a lower bound of
+// the distance from (r, z) to every segment of run q, less a relative margin
+// that covers the rounding of this bound and of the table, and the run's
+// largest segment length.
+__device__ __forceinline__ double blk_lower(const SptBem& b, int q, double r, double z) {
+    const double cr = __ldg(b.blk + q), cz = __ldg(b.blk + b.blk_stride + q), rad = __ldg(b.blk + 2 * b.blk_stride + q);
+    const double dc = sqrt((r - cr) * (r - cr) + (z - cz) * (z - cz));
+    return dc - rad - 1e-9 * (dc + rad);
+}
+__device__ __forceinline__ double blk_lmax(const SptBem& b, int q) { return __ldg(b.blk + 3 * b.blk_stride + q); }
+
 
 // One far-sum round for points r0..r0+np_-1 of the list (np_ <= NP): the
 // node table streams through shared memory in TMA tiles (double buffered);
@@ -505,6 +516,236 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
     __syncthreads();
 }
 
+// Adaptive far sum (SPT_FAR_ADAPTIVE) for points r0..r0+np_-1 of the list.
+// Segments are taken kAdaptSegs at a time (32 runs of SPT_BLOCK_SEGS).  One
+// warp classifies the chunk's runs by the smallest lower-bound distance over
+// the round's points: flagged runs at least ratio_run arclengths away take
+// the 8-point rule over the whole run (list R3), runs whose every segment is
+// at least ratio2 lengths away take Gauss-2 on each segment (R2), the rest
+// (M) are classified segment by segment -- below ratio4 lengths the
+// reference nodes, with an 8-bit mask of the points for which the segment is
+// near (they skip it), below ratio2 Gauss-4, else Gauss-2 (lists L0, L1, L2,
+// in the TMA tile region, which this rule does not use).  The flattened node
+// list L0 | L1 | L2 | R2 | R3 is then evaluated like far_round's tiles,
+// nodes read through L1/L2.  Without run bounds every run is in M.
+constexpr int kAdaptSegs = 1024;
+constexpr int kAdaptRuns = kAdaptSegs / SPT_BLOCK_SEGS;
+static_assert(kAdaptRuns == 32, "one warp classifies a chunk's runs");
+static_assert(3 * kAdaptSegs * sizeof(int) <= 2 * 3 * 256 * sizeof(double), "segment lists must fit the smallest tile region");
+static_assert(kAdaptSegs <= kRound * 256, "near masks must fit the near-flag bytes");
+static_assert(160 <= kWarps * 2 * kRound * 2, "run lists and counts fit the reduction scratch");
+
+template <int NP, int NQ, bool MIX>
+__device__ void far_adaptive(Ctx& c, int r0, int np_, unsigned long long& far_evals) {
+    const SptBem& b = c.bem;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nseg = b.n_seg, nps = b.nodes_per_seg;
+    double* P = c.bpt;
+    int* lists = reinterpret_cast<int*>(c.tiles);  // L0 | L1 | L2, kAdaptSegs each
+    unsigned char* mask = c.nflag;                 // near masks of L0
+    // counts and run lists in the reduction scratch (free until the final reduction)
+    int* s_wc = reinterpret_cast<int*>(c.red);     // [3][kWarps] per-warp level counts
+    int* s_n = s_wc + 24;                          // [3] lengths of L0, L1, L2
+    int* s_rn = s_wc + 27;                         // [3] lengths of R2, R3, M
+    int* R2 = s_wc + 32;
+    int* R3 = s_wc + 64;
+    int* M = s_wc + 96;
+    int* Mcls = s_wc + 128;
+    double pr[NP], pinv[NP], pz[NP], ar[NP], az[NP];
+    float fr[NP], fz[NP], kr[NP], kz[NP], prf[NP], pinvf[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        const int k = r0 + (p < np_ ? p : 0);
+        pr[p] = P[8 * k + 3];
+        pinv[p] = pr[p] > 0.0 ? 1.0 / pr[p] : 0.0;
+        pz[p] = P[8 * k + 4];
+        ar[p] = 0.0;
+        az[p] = 0.0;
+        fr[p] = fz[p] = kr[p] = kz[p] = 0.0f;
+        prf[p] = (float)pr[p];
+        pinvf[p] = (float)pinv[p];
+    }
+    const double r4 = b.ratio4, r2 = b.ratio2;
+    const double* cr = b.coarse;
+    const double* cz = b.coarse + b.coarse_stride;
+    const double* cw = b.coarse + 2 * b.coarse_stride;
+    const bool run_rule = b.blk && b.run_nodes && b.ratio_run > 0.0;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int c0 = 0; c0 < nseg; c0 += kAdaptSegs) {
+        const int q0 = c0 / SPT_BLOCK_SEGS;
+        const int nr = min(kAdaptRuns, (nseg - c0 + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS);
+        if (warp == 0) {
+            const int q = q0 + lane;
+            int cls = -1;  // 3 run rule, 2 Gauss-2 on every segment, 1 no near segment, 0 full test
+            if (lane < nr) {
+                cls = 0;
+                if (b.blk) {
+                    double lb = INFINITY;
+                    for (int p = 0; p < np_; ++p) lb = fmin(lb, blk_lower(b, q, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4]));
+                    const double lm = blk_lmax(b, q);
+                    if (run_rule && __ldg(b.blk + 5 * b.blk_stride + q) != 0.0 &&
+                        lb >= b.ratio_run * __ldg(b.blk + 4 * b.blk_stride + q))
+                        cls = 3;
+                    else if (lb >= r2 * lm) cls = 2;
+                    else if (lb >= r4 * lm) cls = 1;
+                }
+            }
+            const unsigned b3 = __ballot_sync(0xffffffffu, cls == 3);
+            const unsigned b2 = __ballot_sync(0xffffffffu, cls == 2);
+            const unsigned bm = __ballot_sync(0xffffffffu, cls == 0 || cls == 1);
+            if (cls == 3) R3[__popc(b3 & lt)] = q;
+            if (cls == 2) R2[__popc(b2 & lt)] = q;
+            if (cls == 0 || cls == 1) { M[__popc(bm & lt)] = q; Mcls[__popc(bm & lt)] = cls; }
+            if (lane == 0) { s_rn[0] = __popc(b2); s_rn[1] = __popc(b3); s_rn[2] = __popc(bm); }
+            if (lane < 3) s_n[lane] = 0;
+        }
+        __syncthreads();
+        // segment classification of the M runs: one run per warp per wave
+        const int nm = s_rn[2];
+        for (int w0 = 0; w0 < nm; w0 += kWarps) {
+            const int mi = w0 + warp;
+            int lvl = 3;
+            unsigned m = 0;
+            int sg = 0;
+            if (mi < nm) {
+                sg = M[mi] * SPT_BLOCK_SEGS + lane;
+                if (sg < nseg) {
+                    const int cls = Mcls[mi];
+                    const double L = segf(b, 4, sg);
+                    double dmin = INFINITY;
+                    for (int p = 0; p < np_; ++p) {
+                        double proj, dist;
+                        if (seg_near(b, sg, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4], proj, dist)) m |= 1u << p;
+                        dmin = fmin(dmin, dist);
+                    }
+                    if (cls == 1) m = 0, lvl = dmin < r2 * L ? 1 : 2;
+                    else lvl = dmin < r4 * L ? 0 : (dmin < r2 * L ? 1 : 2);
+                }
+            }
+            unsigned bal[3];
+#pragma unroll
+            for (int v = 0; v < 3; ++v) {
+                bal[v] = __ballot_sync(0xffffffffu, lvl == v);
+                if (lane == 0) s_wc[v * kWarps + warp] = __popc(bal[v]);
+            }
+            __syncthreads();
+            if (lvl < 3) {
+                int pos = s_n[lvl] + __popc(bal[lvl] & lt);
+                for (int w = 0; w < warp; ++w) pos += s_wc[lvl * kWarps + w];
+                lists[lvl * kAdaptSegs + pos] = sg;
+                if (lvl == 0) mask[pos] = (unsigned char)m;
+            }
+            __syncthreads();
+            if (tid < 3) {
+                int t = 0;
+                for (int w = 0; w < kWarps; ++w) t += s_wc[tid * kWarps + w];
+                s_n[tid] += t;
+            }
+            __syncthreads();
+        }
+        const int e0 = s_n[0] * nps, e1 = e0 + 4 * s_n[1], e2 = e1 + 2 * s_n[2];
+        const int e3 = e2 + 2 * SPT_BLOCK_SEGS * s_rn[0], e4 = e3 + SPT_RUN_NODES * s_rn[1];
+        for (int q0i = tid; q0i < e4; q0i += kThreads * NQ) {
+            double rq[NQ], zq[NQ], wq[NQ];
+            unsigned mk[NQ];
+            bool in[NQ];
+#pragma unroll
+            for (int j = 0; j < NQ; ++j) {
+                const int q = q0i + j * kThreads;
+                in[j] = q < e4;
+                size_t src = 0;
+                const double *tr = cr, *tz = cz, *tw = cw;
+                mk[j] = 0;
+                if (!in[j]) {
+                    // padding lane: any valid node, not accumulated
+                } else if (q < e0) {
+                    const int li = q / nps;
+                    src = (size_t)lists[li] * nps + (q - li * nps);
+                    tr = b.node;
+                    tz = b.node + b.node_stride;
+                    tw = b.node + 2 * b.node_stride;
+                    mk[j] = mask[li];
+                } else if (q < e1) {
+                    const int i = q - e0;
+                    src = (size_t)lists[kAdaptSegs + (i >> 2)] * 6 + (i & 3);
+                } else if (q < e2) {
+                    const int i = q - e1;
+                    src = (size_t)lists[2 * kAdaptSegs + (i >> 1)] * 6 + 4 + (i & 1);
+                } else if (q < e3) {
+                    const int i = q - e2;
+                    const int sgi = R2[i / (2 * SPT_BLOCK_SEGS)] * SPT_BLOCK_SEGS + ((i & (2 * SPT_BLOCK_SEGS - 1)) >> 1);
+                    if (sgi < nseg) src = (size_t)sgi * 6 + 4 + (i & 1);
+                    else in[j] = false;  // past the last segment of a short final run
+                } else {
+                    const int i = q - e3;
+                    src = (size_t)R3[i / SPT_RUN_NODES] * SPT_RUN_NODES + (i % SPT_RUN_NODES);
+                    tr = b.run_nodes;
+                    tz = b.run_nodes + b.run_stride;
+                    tw = b.run_nodes + 2 * b.run_stride;
+                }
+                rq[j] = __ldg(tr + src);
+                zq[j] = __ldg(tz + src);
+                wq[j] = __ldg(tw + src);
+            }
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+#pragma unroll
+                for (int j = 0; j < NQ; ++j) {
+                    if (p < np_ && in[j] && !((mk[j] >> p) & 1u)) {
+                        const double dz = pz[p] - zq[j];
+                        if (MIX) {
+                            float er, ez;
+                            if (ring_far_f(prf[p], pinvf[p], (float)(pr[p] - rq[j]), (float)(pr[p] + rq[j]), (float)dz,
+                                           (float)rq[j], er, ez)) {
+                                const float w = (float)wq[j];
+                                kahan_add(fr[p], kr[p], w * er);
+                                kahan_add(fz[p], kz[p], w * ez);
+                            } else {
+                                double e64r, e64z;
+                                ring_field_far(pr[p], pinv[p], dz, rq[j], e64r, e64z);
+                                ar[p] = fma(wq[j], e64r, ar[p]);
+                                az[p] = fma(wq[j], e64z, az[p]);
+                            }
+                        } else {
+                            double er, ez;
+                            ring_field_far(pr[p], pinv[p], dz, rq[j], er, ez);
+                            ar[p] = fma(wq[j], er, ar[p]);
+                            az[p] = fma(wq[j], ez, az[p]);
+                        }
+                        ++far_evals;
+                    }
+                }
+            }
+        }
+        __syncthreads();  // the lists are rewritten by the next chunk
+    }
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        if (MIX) {
+            ar[p] += (double)fr[p] - (double)kr[p];
+            az[p] += (double)fz[p] - (double)kz[p];
+        }
+        const double vr = warp_sum(ar[p]);
+        const double vz = warp_sum(az[p]);
+        if (lane == 0) {
+            c.red[warp * 2 * kRound + p] = vr;
+            c.red[warp * 2 * kRound + kRound + p] = vz;
+        }
+    }
+    __syncthreads();
+    if (tid < np_) {
+        double sr = 0.0, sz = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+            sr += c.red[w * 2 * kRound + tid];
+            sz += c.red[w * 2 * kRound + kRound + tid];
+        }
+        const int k = r0 + tid;
+        P[8 * k + 5] = sr + P[8 * k + 7];
+        P[8 * k + 6] = sz + c.fld[3 * k + 2];
+    }
+    __syncthreads();
+}
+
 // ---------------------------------------------------------------------------
 // BEM field of a list of points, in phases.  Records live in c.bpt (8 doubles
 // each: x, y, z, rho_e, z_e, then results); every phase is called by all
@@ -525,9 +766,46 @@ __device__ void bem_closest(Ctx& c, int n, bool frame) {
         const double rho = hypot(x, y);
         double best = INFINITY;
         int bs = 0x7fffffff;
-        for (int s = lane; s < nseg; s += 32) {
-            const double d2 = seg_dist2(b, s, rho, z);
-            if (d2 < best) { best = d2; bs = s; }
+        if (b.blk) {
+            // the run with the smallest lower bound gives an upper bound of the
+            // minimum; only runs whose lower bound does not exceed it are scanned
+            // (each lane still takes its segments in increasing order)
+            const int nblk = (nseg + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS;
+            double lbm = INFINITY;
+            int qm = 0;
+            for (int q = lane; q < nblk; q += 32) {
+                const double lb = blk_lower(b, q, rho, z);
+                if (lb < lbm) { lbm = lb; qm = q; }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ol = __shfl_xor_sync(0xffffffffu, lbm, o);
+                const int oq = __shfl_xor_sync(0xffffffffu, qm, o);
+                if (ol < lbm || (ol == lbm && oq < qm)) { lbm = ol; qm = oq; }
+            }
+            double ub = INFINITY;
+            if (qm * SPT_BLOCK_SEGS + lane < nseg) ub = seg_dist2(b, qm * SPT_BLOCK_SEGS + lane, rho, z);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) ub = fmin(ub, __shfl_xor_sync(0xffffffffu, ub, o));
+            const double ubd = sqrt(ub);
+            for (int q0 = 0; q0 < nblk; q0 += 32) {
+                const bool cand = q0 + lane < nblk && !(blk_lower(b, q0 + lane, rho, z) > ubd);
+                unsigned cm = __ballot_sync(0xffffffffu, cand);
+                while (cm) {
+                    const int j = __ffs(cm) - 1;
+                    cm &= cm - 1;
+                    const int s = (q0 + j) * SPT_BLOCK_SEGS + lane;
+                    if (s < nseg) {
+                        const double d2 = seg_dist2(b, s, rho, z);
+                        if (d2 < best) { best = d2; bs = s; }
+                    }
+                }
+            }
+        } else {
+            for (int s = lane; s < nseg; s += 32) {
+                const double d2 = seg_dist2(b, s, rho, z);
+                if (d2 < best) { best = d2; bs = s; }
+            }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -571,7 +849,15 @@ __device__ void bem_sums(Ctx& c, int n, int* status_flag) {
     for (int k = warp; k < n; k += kWarps) {
         const double re = P[8 * k + 3], ze = P[8 * k + 4];
         double acc_r = 0.0, acc_z = 0.0;
-        for (int s0 = 0; s0 < nseg; s0 += 32) {
+        const int nblk = (nseg + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS;
+        for (int q0 = 0; q0 < nblk; q0 += 32) {
+          // runs that may hold a near segment (every run without the bounds table)
+          const bool cand = q0 + lane < nblk && !(b.blk && blk_lower(b, q0 + lane, re, ze) >= blk_lmax(b, q0 + lane));
+          unsigned cm = __ballot_sync(0xffffffffu, cand);
+          while (cm) {
+            const int jq = __ffs(cm) - 1;
+            cm &= cm - 1;
+            const int s0 = (q0 + jq) * SPT_BLOCK_SEGS;
             const int s = s0 + lane;
             double proj = 0.0, dist = 0.0;
             const bool nr = (s < nseg) && seg_near(b, s, re, ze, proj, dist);
@@ -603,6 +889,7 @@ __device__ void bem_sums(Ctx& c, int n, int* status_flag) {
                 }
                 if (lane == 0) { n_near += 1; n_ring_near += (unsigned long long)cnt * 8; }
             }
+          }
         }
         acc_r = warp_sum(acc_r);
         acc_z = warp_sum(acc_z);
@@ -624,6 +911,14 @@ __device__ void bem_sums(Ctx& c, int n, int* status_flag) {
     bool ok = true;
     for (int r0 = 0; r0 < n; r0 += kRound) {
         const int np_ = min(kRound, n - r0);
+        if (b.far_rule == SPT_FAR_ADAPTIVE) {
+            const bool mix = c.form != SPT_FORM_FP64;
+            if (np_ == 1) mix ? far_adaptive<1, 8, true>(c, r0, np_, far_evals) : far_adaptive<1, 8, false>(c, r0, np_, far_evals);
+            else if (np_ == 2) mix ? far_adaptive<2, 4, true>(c, r0, np_, far_evals) : far_adaptive<2, 4, false>(c, r0, np_, far_evals);
+            else if (np_ <= 4) mix ? far_adaptive<4, 2, true>(c, r0, np_, far_evals) : far_adaptive<4, 2, false>(c, r0, np_, far_evals);
+            else mix ? far_adaptive<8, 1, true>(c, r0, np_, far_evals) : far_adaptive<8, 1, false>(c, r0, np_, far_evals);
+            continue;
+        }
         if (c.form != SPT_FORM_FP64) {  // mixed, and the exact sums of the learned form
             if (np_ == 1)
                 far_round<1, 8, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
@@ -1754,6 +2049,23 @@ int check_bem(const SptBem* b) {
         return fail(SPT_ERR_ARG, "node table must be 16-byte aligned with an even row stride");
     if (b->node_stride < (int64_t)b->n_seg * b->nodes_per_seg || b->seg_stride < b->n_seg)
         return fail(SPT_ERR_ARG, "table strides too small");
+    if (b->far_rule == SPT_FAR_ADAPTIVE) {
+        if (!b->coarse || b->coarse_stride < 6 * (int64_t)b->n_seg)
+            return fail(SPT_ERR_ARG, "adaptive far rule: coarse node table missing or too small");
+        if (!(b->ratio4 >= 1.0) || !(b->ratio2 >= b->ratio4))
+            return fail(SPT_ERR_ARG, "adaptive far rule: need 1 <= ratio4 <= ratio2");
+        const int64_t n_run = (b->n_seg + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS;
+        if (b->blk && b->blk_stride < n_run) return fail(SPT_ERR_ARG, "run bounds table too small");
+        if (b->blk && b->run_nodes && b->ratio_run > 0.0) {
+            // a run at least one arclength away holds no near segment
+            if (!(b->ratio_run >= 1.0)) return fail(SPT_ERR_ARG, "adaptive far rule: ratio_run must be >= 1 (or <= 0: off)");
+            if (b->run_stride < SPT_RUN_NODES * n_run) return fail(SPT_ERR_ARG, "run-node table too small");
+        }
+    } else if (b->far_rule != SPT_FAR_REFERENCE) {
+        return fail(SPT_ERR_ARG, "unknown far rule %d", b->far_rule);
+    }
+    if (b->blk && b->blk_stride < (b->n_seg + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS)
+        return fail(SPT_ERR_ARG, "run bounds table too small");
     return SPT_OK;
 }
 

@@ -107,10 +107,15 @@ FORMS = {"fp64": _lib.FORM_FP64, "mixed": _lib.FORM_MIXED, "surrogate": _lib.FOR
 class Tracer:
     """Persistent-kernel RK45 tracer for one geometry on one device."""
 
-    def __init__(self, geometry, device="cuda", form="fp64", z_max=None, surrogate=None, band=5e-9, spot=0.01):
+    def __init__(self, geometry, device="cuda", form="fp64", z_max=None, surrogate=None, band=5e-9, spot=0.01,
+                 far_rule="reference", ratio4=None, ratio2=None, ratio_run=None):
         """form: "fp64" (plain), "mixed" (float32 + Kahan sums) or "surrogate"
         (mixed, with the learned field outside the `band` [m] around the
-        surface, `spot` of the other points checked against the exact sum)."""
+        surface, `spot` of the other points checked against the exact sum).
+        far_rule: "reference" (every far segment on all its sub-panel nodes)
+        or "adaptive" (whole-segment Gauss-4 / Gauss-2 for segments at least
+        ratio4 / ratio2 lengths away, the 8-node run rule for flagged
+        straight runs at least ratio_run run arclengths away)."""
         torch = _torch()
         self.geometry = geometry
         self.device = torch.device(device)
@@ -118,6 +123,11 @@ class Tracer:
         self.z_max = z_max
         self.geom = geometry.to_struct(z_max=z_max)
         self.tables = geometry.bem_tables(self.device) if geometry.is_bem else None
+        self.far_rule = far_rule
+        self.bem = None
+        if self.tables is not None:
+            kw = {k: v for k, v in (("ratio4", ratio4), ("ratio2", ratio2), ("ratio_run", ratio_run)) if v is not None}
+            self.bem = self.tables.view(far_rule, **kw)
         self._ws = None
         self.counters = torch.zeros(_lib.N_COUNTERS, dtype=torch.int64, device=self.device)
         self.surrogate = None
@@ -155,7 +165,7 @@ class Tracer:
     def workspace(self, state, params):
         torch = _torch()
         nbytes = ctypes.c_int64(0)
-        bem = ctypes.byref(self.tables.struct) if self.tables is not None else None
+        bem = ctypes.byref(self.bem) if self.bem is not None else None
         _lib.check(_lib.lib().spt_trace_workspace_bytes(ctypes.byref(state), ctypes.byref(params),
                                                         ctypes.byref(self.geom), bem, ctypes.byref(nbytes)),
                    "spt_trace_workspace_bytes")
@@ -171,7 +181,7 @@ class Tracer:
         ws = self.workspace(st, params)
         if stream is None:
             stream = torch.cuda.current_stream(self.device)
-        bem = ctypes.byref(self.tables.struct) if self.tables is not None else None
+        bem = ctypes.byref(self.bem) if self.bem is not None else None
         _lib.check(_lib.lib().spt_trace(ctypes.byref(st), ctypes.byref(params), ctypes.byref(self.geom), bem,
                                         ctypes.c_void_p(ws.data_ptr()), ws.numel(),
                                         ctypes.c_void_p(stream.cuda_stream)), "spt_trace")
@@ -300,7 +310,7 @@ class TraceRecords:
 
 
 def accel(geometry, pos, active, charge, mass, group_sizes, charge_to_mass, plummer_radius, device="cuda",
-          form="fp64", coulomb_constant=COULOMB_CONSTANT):
+          form="fp64", coulomb_constant=COULOMB_CONSTANT, far_rule="reference"):
     """One stage evaluation through spt_accel; returns acc [N, 3] (torch)."""
     torch = _torch()
     sizes = np.asarray(group_sizes, dtype=np.int64)
@@ -331,20 +341,21 @@ def accel(geometry, pos, active, charge, mass, group_sizes, charge_to_mass, plum
     tables = geometry.bem_tables(d) if geometry.is_bem else None
     stream = torch.cuda.current_stream(d)
     _lib.check(_lib.lib().spt_accel(ctypes.byref(a), ctypes.byref(geom),
-                                    ctypes.byref(tables.struct) if tables is not None else None,
+                                    ctypes.byref(tables.view(far_rule)) if tables is not None else None,
                                     ctypes.c_void_p(stream.cuda_stream)), "spt_accel")
     return torch.stack(out, dim=-1)
 
 
-def bem_field(tables, points, form="fp64"):
+def bem_field(tables, points, form="fp64", far_rule="reference", **rule_kw):
     """Perturbation field of a BEM solution at points [N, 3] (spt_bem_field)."""
+    view = tables.view(far_rule, **rule_kw)
     torch = _torch()
     p = _as_dev(points, torch.float64, tables.seg.device).reshape(-1, 3)
     x, y, z = (p[:, k].contiguous() for k in range(3))
     out = [torch.empty_like(x) for _ in range(3)]
     stream = torch.cuda.current_stream(tables.seg.device)
     _lib.check(_lib.lib().spt_bem_field(x.data_ptr(), y.data_ptr(), z.data_ptr(), x.numel(),
-                                        ctypes.byref(tables.struct), FORMS[form] if isinstance(form, str) else form,
+                                        ctypes.byref(view), FORMS[form] if isinstance(form, str) else form,
                                         out[0].data_ptr(), out[1].data_ptr(), out[2].data_ptr(),
                                         ctypes.c_void_p(stream.cuda_stream)), "spt_bem_field")
     return torch.stack(out, dim=-1)
@@ -402,7 +413,7 @@ def sg_param_shapes():
     return PARAM_SHAPES
 
 
-def surrogate_field(tables, binding, points):
+def surrogate_field(tables, binding, points, far_rule="reference"):
     """Learned-form perturbation field at points [N, 3] (spt_surrogate_field):
     the surrogate outside the binding's band, exact inside it and for its
     spot checks."""
@@ -413,7 +424,7 @@ def surrogate_field(tables, binding, points):
     prm = binding.fill(_lib.SptTraceParams())
     stream = torch.cuda.current_stream(tables.seg.device)
     _lib.check(_lib.lib().spt_surrogate_field(x.data_ptr(), y.data_ptr(), z.data_ptr(), x.numel(),
-                                              ctypes.byref(tables.struct), ctypes.byref(prm), out[0].data_ptr(),
+                                              ctypes.byref(tables.view(far_rule)), ctypes.byref(prm), out[0].data_ptr(),
                                               out[1].data_ptr(), out[2].data_ptr(),
                                               ctypes.c_void_p(stream.cuda_stream)), "spt_surrogate_field")
     return torch.stack(out, dim=-1)

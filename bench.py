@@ -80,6 +80,18 @@ def build_workload(name, rank=0):
     raise ValueError(name)
 
 
+def first_groups(data, n):
+    """The workload cut to its first n emission groups (a smaller case of the
+    same kernel, for profiling)."""
+    sizes = np.asarray(data["group_sizes"])
+    if n is None or n >= len(sizes):
+        return data
+    k = int(sizes[:n].sum())
+    out = {key: (v[:k] if isinstance(v, np.ndarray) and v.shape[:1] == (int(sizes.sum()),) else v) for key, v in data.items()}
+    out["group_sizes"] = sizes[:n]
+    return out
+
+
 def particle_arrays(data):
     from bem_b200.constants import ELEMENTARY_CHARGE, SPEED_OF_LIGHT, ev_to_kg
     m = ev_to_kg(510998.95069)
@@ -246,9 +258,12 @@ def run_gpu(args, rank, world):
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
     wl = build_workload(args.workload, rank)
+    if args.groups:
+        wl["data"] = first_groups(wl["data"], args.groups)
+        wl["config"] = dict(wl["config"], groups=args.groups, workload=wl["config"]["workload"] + f" (first {args.groups} groups)")
     pos, vel, tb, q, m, cm = particle_arrays(wl["data"])
     sizes = wl["data"]["group_sizes"]
-    tracer = engine.Tracer(wl["geometry"], device=dev, form=args.form, z_max=wl["z_max"])
+    tracer = engine.Tracer(wl["geometry"], device=dev, form=args.form, z_max=wl["z_max"], far_rule=args.far_rule)
     batch = engine.GroupBatch(pos, vel, tb, q, m, sizes, device=dev)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
@@ -351,7 +366,10 @@ def main():
     ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2", "c3", "c4"])
     ap.add_argument("--attempts", type=int, default=16, help="RK45 attempts per group per step")
     ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--far-rule", default="reference", choices=["reference", "adaptive"],
+                    help="far-field quadrature of the BEM sum (adaptive: whole-segment Gauss-4/2 when distant)")
     ap.add_argument("--cpu-attempts", type=int, default=16)
+    ap.add_argument("--groups", type=int, default=None, help="first N emission groups only (profiling a smaller case)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -383,7 +401,7 @@ def main():
         metric=METRIC, value=r["value"], unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
         ms_per_step=mean_ms, higher_is_better=True, scaling="weak", vs_baseline=None,
         dtype="f64" if args.form == "fp64" else "f32+f64", data="synthetic (seeded samplers, workloads.py)",
-        config=dict(r["config"], form=args.form, attempts_per_step=args.attempts, parallelism=f"groups x {world} GPUs",
+        config=dict(r["config"], form=args.form, far_rule=args.far_rule, attempts_per_step=args.attempts, parallelism=f"groups x {world} GPUs",
                     l2="flushed between steps (256 MiB write); each step timed alone with CUDA events"),
         clocks=r["clocks"], gpu_launches=args.steps,
         roofline=dict(bound="fp64", achieved=r["achieved"], peak=r["fp64_peak"], unit="TFLOP/s",

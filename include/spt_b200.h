@@ -114,7 +114,46 @@ typedef struct {
     const double* node;
     double gauss8_x[8];      /* Gauss-Legendre 8-point nodes/weights on [-1, 1] */
     double gauss8_w[8];
+    /* Far-field rule (no counterpart in the reference, which always uses the
+     * first): SPT_FAR_REFERENCE sums every far segment over its
+     * nodes_per_seg nodes; SPT_FAR_ADAPTIVE classifies each segment, per
+     * round of up to 8 evaluation points, by the smallest distance / length
+     * ratio over the round: below ratio4 the reference nodes, below ratio2
+     * the 4-point Gauss rule over the whole segment, else the 2-point rule.
+     * `coarse` holds 3 rows (rho_q, z_q, w_q) of coarse_stride doubles with
+     * 6 nodes per segment: the 4 Gauss-4 nodes, then the 2 Gauss-2 nodes.
+     * ratio4 >= 1 (coarse segments are never near), ratio2 >= ratio4. */
+    int32_t far_rule;
+    int32_t reserved;
+    double ratio4;
+    double ratio2;
+    const double* coarse;
+    int64_t coarse_stride;
+    /* Optional bounds of each run of SPT_BLOCK_SEGS consecutive segments,
+     * 6 rows of blk_stride doubles: centre rho, centre z, radius (largest
+     * distance from the centre to an endpoint of the run), largest segment
+     * length, arclength of the run, and 1 where the run may take the run
+     * rule below (else 0).  With it the closest-segment search, the near
+     * test and the adaptive classification skip runs that cannot qualify
+     * (results are unchanged); NULL scans every segment. */
+    const double* blk;
+    int64_t blk_stride;
+    /* Run rule (adaptive far rule with blk only): a run flagged in blk row 5
+     * whose lower-bound distance over the round is at least ratio_run times
+     * its arclength takes the 8-point Gauss rule over the whole run.
+     * run_nodes holds 3 rows (rho_q, z_q, w_q) of run_stride doubles, 8 nodes
+     * per run.  ratio_run <= 0 turns the rule off. */
+    double ratio_run;
+    const double* run_nodes;
+    int64_t run_stride;
 } SptBem;
+
+#define SPT_RUN_NODES 8
+
+#define SPT_BLOCK_SEGS 32
+
+#define SPT_FAR_REFERENCE 0
+#define SPT_FAR_ADAPTIVE 1
 
 /* Particle and per-group integrator state, in/out. Groups are contiguous
  * particle ranges [group_offset[g], group_offset[g+1]). */

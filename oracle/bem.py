@@ -12,6 +12,7 @@ from scipy import special
 
 GAUSS4_X, GAUSS4_W = np.polynomial.legendre.leggauss(4)  # bem/axisymmetric.py:98
 GAUSS8_X, GAUSS8_W = np.polynomial.legendre.leggauss(8)  # bem/axisymmetric.py:94
+GAUSS2_X, GAUSS2_W = np.polynomial.legendre.leggauss(2)  # adaptive far rule only (not in the reference)
 
 
 def ellip_k_e_complement(p):
@@ -103,8 +104,113 @@ def _near_segment_sum(rho_e, z_e, seg, sigma, j, s0, d):
     return np.sum(w * er), np.sum(w * ez)
 
 
-def field(points, profile, sigma, n_subdiv=8, chunk=256):
-    """bem/axisymmetric.py:501-605 -- E = -grad S[sigma] at points (..., 3)."""
+def whole_segment_nodes(profile, sigma, gx, gw):
+    """Gauss rule (gx, gw) over each whole segment: (rho_q, z_q, area_q *
+    sigma_q), each [n_seg, len(gx)].  Used by the adaptive far rule."""
+    profile = np.asarray(profile, dtype=float)
+    sigma = np.asarray(sigma, dtype=float)
+    p0, p1 = profile[:-1], profile[1:]
+    length = np.linalg.norm(p1 - p0, axis=-1)
+    t = 0.5 * (np.asarray(gx) + 1.0)[None, :]
+    r = p0[:, :1] + t * (p1[:, :1] - p0[:, :1])
+    z = p0[:, 1:] + t * (p1[:, 1:] - p0[:, 1:])
+    w = 2.0 * np.pi * r * (length[:, None] * 0.5 * np.asarray(gw)[None, :])
+    return r, z, w * (sigma[:-1, None] + t * (sigma[1:, None] - sigma[:-1, None]))
+
+
+def run_rule_nodes(profile, sigma, block=32, n=8):
+    """Run rule (adaptive far rule, not in the reference): for each run of
+    `block` consecutive segments, n nodes at the Gauss points of its
+    arclength and product-integration weights w_i = integral of
+    sigma 2 pi rho l_i over the run (l_i the Lagrange polynomial of node i).
+    Returns (rho [n_run, n], z, w, centre [n_run, 2], radius, arclength)."""
+    profile = np.asarray(profile, dtype=float)
+    sigma = np.asarray(sigma, dtype=float)
+    nseg = len(profile) - 1
+    length = np.linalg.norm(profile[1:] - profile[:-1], axis=-1)
+    s_node = np.concatenate([[0.0], np.cumsum(length)])
+    gx, _ = np.polynomial.legendre.leggauss(n)
+    g5x, g5w = np.polynomial.legendre.leggauss(5)
+    nrun = (nseg + block - 1) // block
+    R, Z, W = np.zeros((nrun, n)), np.zeros((nrun, n)), np.zeros((nrun, n))
+    cen, rad, arc = np.zeros((nrun, 2)), np.zeros(nrun), np.zeros(nrun)
+    for q in range(nrun):
+        a, b = q * block, min((q + 1) * block, nseg)
+        pts = profile[a:b + 1]
+        cen[q] = 0.5 * (pts.min(axis=0) + pts.max(axis=0))
+        rad[q] = np.sqrt(((pts - cen[q]) ** 2).sum(axis=-1)).max()
+        arc[q] = s_node[b] - s_node[a]
+        sq = s_node[a] + 0.5 * (gx + 1.0) * arc[q]
+        for i, sv in enumerate(sq):
+            j = min(max(int(np.searchsorted(s_node, sv, side="right")) - 1, a), b - 1)
+            t = (sv - s_node[j]) / length[j]
+            R[q, i] = profile[j, 0] + t * (profile[j + 1, 0] - profile[j, 0])
+            Z[q, i] = profile[j, 1] + t * (profile[j + 1, 1] - profile[j, 1])
+        for j in range(a, b):
+            t = 0.5 * (g5x + 1.0)
+            sv = s_node[j] + t * length[j]
+            f = (2.0 * np.pi * (profile[j, 0] + t * (profile[j + 1, 0] - profile[j, 0]))
+                 * (sigma[j] + t * (sigma[j + 1] - sigma[j])) * 0.5 * length[j] * g5w)
+            for i in range(n):
+                lag = np.ones_like(sv)
+                for m in range(n):
+                    if m != i:
+                        lag *= (sv - sq[m]) / (sq[i] - sq[m])
+                W[q, i] += np.sum(lag * f)
+    return R, Z, W, cen, rad, arc
+
+
+def _run_override(er_s, ez_s, rho_e, z_e, runs, run_flags, ratio_run, round_size, block=32):
+    """Run rule: for each round, a flagged run whose bounding circle is at
+    least ratio_run arclengths from every point of the round contributes its
+    n-node sum (kept in its first segment's slot, the others zeroed)."""
+    R, Z, W, cen, rad, arc = runs
+    nseg = er_s.shape[1]
+    for a in range(0, len(rho_e), round_size):
+        b = min(a + round_size, len(rho_e))
+        lb = np.full(len(arc), np.inf)
+        for p in range(a, b):
+            lb = np.minimum(lb, np.hypot(rho_e[p] - cen[:, 0], z_e[p] - cen[:, 1]) - rad)
+        for q in np.nonzero(np.asarray(run_flags, dtype=bool) & (lb >= ratio_run * arc))[0]:
+            s0, s1 = q * block, min((q + 1) * block, nseg)
+            for p in range(a, b):
+                er, ez = ring_field(rho_e[p], z_e[p] - Z[q], R[q])
+                er_s[p, s0:s1] = 0.0
+                ez_s[p, s0:s1] = 0.0
+                er_s[p, s0] = np.sum(W[q] * er)
+                ez_s[p, s0] = np.sum(W[q] * ez)
+
+
+def _adaptive_override(er_s, ez_s, rho_e, z_e, dist, seg, coarse, ratio4, ratio2, round_size):
+    """The adaptive far rule: for each round of `round_size` consecutive
+    points, a segment whose smallest distance over the round is at least
+    ratio4 lengths takes the whole-segment Gauss-4 rule, at least ratio2 the
+    Gauss-2 rule (replacing the sub-panel sums for every point of the round)."""
+    L = seg["length"]
+    (r4, z4, w4), (r2, z2, w2) = coarse
+    for a in range(0, len(rho_e), round_size):
+        b = min(a + round_size, len(rho_e))
+        dmin = dist[a:b].min(axis=0)
+        for lvl, (rq, zq, wq) in ((1, (r4, z4, w4)), (2, (r2, z2, w2))):
+            sel = (dmin >= ratio4 * L) & (dmin < ratio2 * L) if lvl == 1 else dmin >= ratio2 * L
+            js = np.nonzero(sel)[0]
+            if len(js) == 0:
+                continue
+            for p in range(a, b):
+                er, ez = ring_field(rho_e[p], z_e[p] - zq[js], rq[js])
+                er_s[p, js] = np.sum(wq[js] * er, axis=-1)
+                ez_s[p, js] = np.sum(wq[js] * ez, axis=-1)
+
+
+def field(points, profile, sigma, n_subdiv=8, chunk=256, far_rule="reference", ratio4=8.0, ratio2=300.0,
+          round_size=8, run_flags=None, ratio_run=4.0):
+    """bem/axisymmetric.py:501-605 -- E = -grad S[sigma] at points (..., 3).
+
+    far_rule="adaptive" swaps the sub-panel sums of distant segments for the
+    whole-segment rules of ``_adaptive_override`` (chunk must be a multiple
+    of round_size so rounds are consecutive points of the input), and, with
+    ``run_flags`` (which runs of 32 segments may take it), distant flagged
+    runs for the run rule of ``_run_override``."""
     points = np.asarray(points, dtype=float)
     shape = points.shape
     flat = points.reshape(-1, 3)
@@ -114,6 +220,13 @@ def field(points, profile, sigma, n_subdiv=8, chunk=256):
     wq = aq * sq
     nseg = len(seg["p0"])
     per = len(rq) // nseg
+    if far_rule == "adaptive":
+        coarse = (whole_segment_nodes(profile, sigma, GAUSS4_X, GAUSS4_W),
+                  whole_segment_nodes(profile, sigma, GAUSS2_X, GAUSS2_W))
+        runs = run_rule_nodes(profile, sigma) if run_flags is not None else None
+        assert chunk % round_size == 0
+    elif far_rule != "reference":
+        raise ValueError(far_rule)
     out = np.empty_like(flat)
     for c0 in range(0, len(flat), chunk):
         f = flat[c0:c0 + chunk]
@@ -133,6 +246,10 @@ def field(points, profile, sigma, n_subdiv=8, chunk=256):
         along = np.sum(delta * seg["unit"][None, :, :], axis=-1)
         proj = np.clip(along, 0.0, seg["length"][None, :])
         dist = np.linalg.norm(delta - proj[..., None] * seg["unit"][None, :, :], axis=-1)
+        if far_rule == "adaptive":
+            _adaptive_override(er_s, ez_s, rho_e, z, dist, seg, coarse, ratio4, ratio2, round_size)
+            if runs is not None:
+                _run_override(er_s, ez_s, rho_e, z, runs, run_flags, ratio_run, round_size)
         pi, si = np.nonzero(dist < seg["length"][None, :])
         for p, s in zip(pi, si):
             d = max(dist[p, s], 1e-15 * seg["length"][s])

@@ -45,13 +45,13 @@ def oracle_trace(spec, pos0, vel0, tb, t_max, rtol, atol, z_max, max_attempts=No
 
 
 def device_trace(spec, pos0, vel0, tb, t_max, rtol, atol, z_max, max_attempts=None, log_capacity=4096,
-                 form="fp64"):
+                 form="fp64", far_rule="reference"):
     import torch
     from bem_b200 import engine
 
     G, E, _ = pos0.shape
     geo = device_geometry(spec)
-    tr = engine.Tracer(geo, form=form, z_max=z_max)
+    tr = engine.Tracer(geo, form=form, z_max=z_max, far_rule=far_rule)
     batch = engine.GroupBatch(pos0.reshape(-1, 3), vel0.reshape(-1, 3), tb.reshape(-1), np.full(G * E, Q_E),
                               np.full(G * E, M_E), [E] * G)
     if max_attempts is None:

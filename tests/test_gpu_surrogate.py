@@ -4,7 +4,7 @@ Trained here (small) on the post-tip fixture geometry.
 
 Checks: the in-kernel network agrees with the standalone one
 (FieldSurrogate.predict); with every point exact (band covering all, or
-spot = 1) the learned form reproduces the mixed form bit for bit; a trace
+spot = 1) the learned form reproduces the mixed form; a trace
 driven by the surrogate stays close to the exact one and does a fraction of
 its ring evaluations (the ablation)."""
 
@@ -92,7 +92,9 @@ def test_band_covering_everything_is_the_exact_field(post):
     bind = engine.SurrogateBinding(model, band=1.0, spot=0.0)
     E = engine.surrogate_field(tables, bind, pts).cpu().numpy()
     ref = engine.bem_field(tables, pts, form="mixed").cpu().numpy()
-    np.testing.assert_array_equal(E, ref)
+    # same device code in another kernel: equal up to the compiler's
+    # contraction choices in the float32 sums (the network is off by percents)
+    np.testing.assert_allclose(E, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
     assert bind.stats()[:3] == (0, len(pts), 0)
 
 
@@ -125,7 +127,8 @@ def test_spot_checks_record_the_surrogate_error(post):
     tables = geo.bem_tables("cuda")
     bind = engine.SurrogateBinding(model, band=0.0, spot=1.0)
     E = engine.surrogate_field(tables, bind, pts).cpu().numpy()
-    np.testing.assert_array_equal(E, engine.bem_field(tables, pts, form="mixed").cpu().numpy())
+    ref = engine.bem_field(tables, pts, form="mixed").cpu().numpy()
+    np.testing.assert_allclose(E, ref, rtol=1e-12, atol=1e-12 * np.abs(ref).max())
     n_sur, n_band, n_spot, err = bind.stats()
     assert (n_sur, n_band, n_spot) == (0, 0, len(pts))
     # the recorded maximum is the network's error against the exact field
