@@ -1213,11 +1213,13 @@ __device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
 // form: separations are taken in float64 (nearby particles far from the
 // origin), then the rest in float32 with Kahan-compensated sums.
 template <bool MIX, typename SRC>
-__device__ __forceinline__ void pair_sum(const Ctx& c, int E, double xi, double yi, double zi, double qk, SRC src,
-                                         double& fx, double& fy, double& fz) {
+__device__ __forceinline__ void pair_sum(const Ctx& c, int E, int j0, int jstep, double xi, double yi, double zi,
+                                         double qk, SRC src, double& fx, double& fy, double& fz) {
+    // sources j0, j0 + jstep, ... (the callers split one target's sources over
+    // the lanes of a warp and add the partial sums)
     if (!MIX) {
         double ax = 0.0, ay = 0.0, az = 0.0;
-        for (int j = 0; j < E; ++j) {
+        for (int j = j0; j < E; j += jstep) {
             if (!c.live[j]) continue;
             double x, y, z, q;
             src(j, x, y, z, q);
@@ -1233,7 +1235,7 @@ __device__ __forceinline__ void pair_sum(const Ctx& c, int E, double xi, double 
     } else {
         float ax = 0.f, ay = 0.f, az = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
         const float soft2 = (float)c.soft2;
-        for (int j = 0; j < E; ++j) {
+        for (int j = j0; j < E; j += jstep) {
             if (!c.live[j]) continue;
             double x, y, z, q;
             src(j, x, y, z, q);
@@ -1249,6 +1251,12 @@ __device__ __forceinline__ void pair_sum(const Ctx& c, int E, double xi, double 
         fy = (double)ay - (double)cy;
         fz = (double)az - (double)cz;
     }
+}
+
+// sum of v over the T consecutive lanes of a lane group (T a power of two <= 32)
+__device__ __forceinline__ double group_sum(double v, int T) {
+    for (int o = T >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
 }
 
 // ---------------------------------------------------------------------------
@@ -1331,12 +1339,73 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
         __syncthreads();
     }
 
-    // 3. per particle: field + pair sums
+    // 3. per particle: field + pair sums.  Each target's sources are split
+    // over T lanes of a warp (T = 256 / E rounded down to a power of two, at
+    // most 32), whose partial sums are added with shuffles.
+    int T = 1;
+    while (T < 32 && T * 2 * E <= kThreads) T *= 2;
+    const int per_pass = kThreads / T;
+    const int sub = tid & (T - 1);
     unsigned long long pairs = 0;
-    for (int i = tid; i < E; i += kThreads) {
+    for (int base = 0; base < E; base += per_pass) {
+        const int i = base + tid / T;
+        const bool act = i < E && c.live[i];
         double ax = 0.0, ay = 0.0, az = 0.0;
-        if (c.live[i]) {
-            const double xi = sx[i], yi = sy[i], zi = sz[i];
+        double fcx = 0.0, fcy = 0.0, fcz = 0.0, fix = 0.0, fiy = 0.0, fiz = 0.0;
+        const bool mix = c.form != SPT_FORM_FP64;
+        const int ii = i < E ? i : 0;
+        const double xi = sx[ii], yi = sy[ii], zi = sz[ii];
+        const double qk = c.kc * c.q[ii];
+        if (act) {
+            if (E > 1) {
+                auto real = [&](int j, double& x, double& y, double& z, double& q) {
+                    x = sx[j]; y = sy[j]; z = sz[j]; q = c.q[j];
+                };
+                if (mix) pair_sum<true>(c, E, sub, T, xi, yi, zi, qk, real, fcx, fcy, fcz);
+                else pair_sum<false>(c, E, sub, T, xi, yi, zi, qk, real, fcx, fcy, fcz);
+                if (sub == 0) pairs += E;
+            }
+            if (KIND == SPT_GEOM_FLAT && g.has_image) {
+                const double zimg = -2.0 * g.z0;
+                auto mirror = [&](int j, double& x, double& y, double& z, double& q) {
+                    x = sx[j]; y = sy[j]; z = zimg - sz[j]; q = -c.q[j];
+                };
+                if (mix) pair_sum<true>(c, E, sub, T, xi, yi, zi, qk, mirror, fix, fiy, fiz);
+                else pair_sum<false>(c, E, sub, T, xi, yi, zi, qk, mirror, fix, fiy, fiz);
+                if (sub == 0) pairs += E;
+            } else if (three_img) {
+                const double zc = (KIND == SPT_GEOM_POST_BEM) ? g.L : 0.0;
+                const double pz0 = (KIND == SPT_GEOM_POST_BEM) ? g.L + g.z0 : g.z0;
+                const double zl = zi - zc;
+                double s1x, s1y, s1z, s2x, s2y, s2z, s3x, s3y, s3z;
+                auto sphere = [&](int j, double& x, double& y, double& z, double& q) {
+                    x = c.img[j]; y = c.img[E + j]; z = c.img[2 * E + j]; q = c.img[3 * E + j];
+                };
+                auto plane = [&](int j, double& x, double& y, double& z, double& q) {
+                    x = sx[j]; y = sy[j]; z = -2.0 * pz0 - (sz[j] - zc); q = -c.q[j];
+                };
+                auto plane_sphere = [&](int j, double& x, double& y, double& z, double& q) {
+                    x = c.img[j]; y = c.img[E + j]; z = -2.0 * pz0 - c.img[2 * E + j]; q = -c.img[3 * E + j];
+                };
+                if (mix) {
+                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, sphere, s1x, s1y, s1z);
+                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, plane, s2x, s2y, s2z);
+                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, plane_sphere, s3x, s3y, s3z);
+                } else {
+                    pair_sum<false>(c, E, sub, T, xi, yi, zl, qk, sphere, s1x, s1y, s1z);
+                    pair_sum<false>(c, E, sub, T, xi, yi, zl, qk, plane, s2x, s2y, s2z);
+                    pair_sum<false>(c, E, sub, T, xi, yi, zl, qk, plane_sphere, s3x, s3y, s3z);
+                }
+                fix = (s1x + s2x) + s3x;
+                fiy = (s1y + s2y) + s3y;
+                fiz = (s1z + s2z) + s3z;
+                if (sub == 0) pairs += 3 * E;
+            }
+        }
+        // every lane takes part in the shuffles (inactive ones add zeros)
+        fcx = group_sum(fcx, T); fcy = group_sum(fcy, T); fcz = group_sum(fcz, T);
+        fix = group_sum(fix, T); fiy = group_sum(fiy, T); fiz = group_sum(fiz, T);
+        if (act && sub == 0) {
             double ex, ey, ez;
             if (KIND == SPT_GEOM_FLAT) {
                 ex = 0.0; ey = 0.0; ez = (zi >= 0.0) ? g.E_gun : 0.0;
@@ -1359,62 +1428,16 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
                 ey = w * ny + (1.0 - w) * 0.0;
                 ez = w * nz + (1.0 - w) * fz;
             }
-            const double qk = c.kc * c.q[i];
-            const bool mix = c.form != SPT_FORM_FP64;
-            double fcx = 0.0, fcy = 0.0, fcz = 0.0;
-            if (E > 1) {
-                auto real = [&](int j, double& x, double& y, double& z, double& q) {
-                    x = sx[j]; y = sy[j]; z = sz[j]; q = c.q[j];
-                };
-                if (mix) pair_sum<true>(c, E, xi, yi, zi, qk, real, fcx, fcy, fcz);
-                else pair_sum<false>(c, E, xi, yi, zi, qk, real, fcx, fcy, fcz);
-                pairs += E;
-            }
-            double fix = 0.0, fiy = 0.0, fiz = 0.0;
-            if (KIND == SPT_GEOM_FLAT && g.has_image) {
-                const double zimg = -2.0 * g.z0;
-                auto mirror = [&](int j, double& x, double& y, double& z, double& q) {
-                    x = sx[j]; y = sy[j]; z = zimg - sz[j]; q = -c.q[j];
-                };
-                if (mix) pair_sum<true>(c, E, xi, yi, zi, qk, mirror, fix, fiy, fiz);
-                else pair_sum<false>(c, E, xi, yi, zi, qk, mirror, fix, fiy, fiz);
-                pairs += E;
-            } else if (three_img) {
-                const double zc = (KIND == SPT_GEOM_POST_BEM) ? g.L : 0.0;
-                const double pz0 = (KIND == SPT_GEOM_POST_BEM) ? g.L + g.z0 : g.z0;
-                const double zl = zi - zc;
-                double s1x, s1y, s1z, s2x, s2y, s2z, s3x, s3y, s3z;
-                auto sphere = [&](int j, double& x, double& y, double& z, double& q) {
-                    x = c.img[j]; y = c.img[E + j]; z = c.img[2 * E + j]; q = c.img[3 * E + j];
-                };
-                auto plane = [&](int j, double& x, double& y, double& z, double& q) {
-                    x = sx[j]; y = sy[j]; z = -2.0 * pz0 - (sz[j] - zc); q = -c.q[j];
-                };
-                auto plane_sphere = [&](int j, double& x, double& y, double& z, double& q) {
-                    x = c.img[j]; y = c.img[E + j]; z = -2.0 * pz0 - c.img[2 * E + j]; q = -c.img[3 * E + j];
-                };
-                if (mix) {
-                    pair_sum<true>(c, E, xi, yi, zl, qk, sphere, s1x, s1y, s1z);
-                    pair_sum<true>(c, E, xi, yi, zl, qk, plane, s2x, s2y, s2z);
-                    pair_sum<true>(c, E, xi, yi, zl, qk, plane_sphere, s3x, s3y, s3z);
-                } else {
-                    pair_sum<false>(c, E, xi, yi, zl, qk, sphere, s1x, s1y, s1z);
-                    pair_sum<false>(c, E, xi, yi, zl, qk, plane, s2x, s2y, s2z);
-                    pair_sum<false>(c, E, xi, yi, zl, qk, plane_sphere, s3x, s3y, s3z);
-                }
-                fix = (s1x + s2x) + s3x;
-                fiy = (s1y + s2y) + s3y;
-                fiz = (s1z + s2z) + s3z;
-                pairs += 3 * E;
-            }
             const double mi = c.m[i];
             ax = (c.cm * ex + fcx / mi) + fix / mi;
             ay = (c.cm * ey + fcy / mi) + fiy / mi;
             az = (c.cm * ez + fcz / mi) + fiz / mi;
         }
-        out[i] = ax;
-        out[E + i] = ay;
-        out[2 * E + i] = az;
+        if (i < E && sub == 0) {
+            out[i] = ax;
+            out[E + i] = ay;
+            out[2 * E + i] = az;
+        }
     }
     c.cnt[SPT_CNT_PAIR_EVALS] += pairs;
     __syncthreads();

@@ -229,23 +229,65 @@ __device__ __forceinline__ void ellip_ke_f_fixed(float p, float& K, float& E) {
     E = K * (1.0f - S);
 }
 
-// float32 ring field for the far sum of the mixed form, branch free so that
-// several evaluations interleave.  dr = rho - a and sr = rho + a are formed in
-// float64 by the caller (rho and a are close near a wall), then rounded.
-// K and E come from a fixed six-step float AGM (converged for p >= 1e-3).
-// Returns false -- the caller then uses the float64 ring_field_far -- when
-// p = d2/D < 1e-3 (m > 0.999, where K(m -> 1) needs the digits) or when the
-// point is within 1e-2 of the node distance from the axis (the radial
-// component cancels there and is scaled by 1/rho; the Taylor branch needs
-// (a^2+z^2)^-3.5, beyond float range for nm rings).
+// float32 unit-ring field near the axis: with r^2 = a^2 + z^2, x = rho / r and
+// t = z / r, the potential of the ring expands in Legendre polynomials of t
+// (the z-derivatives of the on-axis potential 1 / (4 pi r)):
+//   E_rho = 1/(4 pi r^2) sum_{k>=1} (-1)^(k+1) c_k x^(2k-1) P_2k(t)
+//   E_z   = 1/(4 pi r^2) sum_{k>=0} (-1)^k c_(k+1) x^(2k) P_(2k+1)(t)
+// with c_k = 2k binom(2k, k) / 4^k.  Every term is O(1): no cancellation and
+// no overflow for nm rings.  Terms through P_17; for x^2 < 0.09 the remainder
+// is below 2e-8 of 1/(4 pi r^2).
+__device__ __forceinline__ void ring_axis_f(float rho, float z, float a, float& er, float& ez) {
+    constexpr float ck[10] = {0.0f, 1.0f, 1.5f, 1.875f, 2.1875f, 2.4609375f, 2.70703125f, 2.9326171875f,
+                              3.14208984375f, 3.338470458984375f};
+    const float r2 = fmaf(a, a, z * z);
+    const float ir = rsqrtf(r2);
+    const float x = rho * ir, t = z * ir, x2 = x * x;
+    float pm = 1.0f, pn = t;  // P_(n-1), P_n
+    float sr = 0.0f, sz = t;  // E_z term k = 0: c_1 P_1
+    float xo = x, xe = x2;    // x^(2k-1) for the next E_rho term, x^(2k) for the next E_z term
+#pragma unroll
+    for (int n = 1; n <= 16; ++n) {
+        const float pnext = ((float)(2 * n + 1) * t * pn - (float)n * pm) * (1.0f / (float)(n + 1));
+        pm = pn;
+        pn = pnext;
+        if ((n + 1) % 2 == 0) {
+            const int k = (n + 1) / 2;
+            const float term = ck[k] * xo * pn;
+            sr = (k % 2 == 1) ? sr + term : sr - term;
+            xo *= x2;
+        } else {
+            const int k = n / 2;
+            const float term = ck[k + 1] * xe * pn;
+            sz = (k % 2 == 0) ? sz + term : sz - term;
+            xe *= x2;
+        }
+    }
+    const float s = 0.07957747154594767f * (ir * ir);  // 1/(4 pi r^2)
+    er = s * sr;
+    ez = s * sz;
+}
+
+// float32 ring field for the far sum of the mixed form.  dr = rho - a and
+// sr = rho + a are formed in float64 by the caller (rho and a are close near
+// a wall), then rounded.  Near the axis (rho^2 < 0.09 (a^2 + z^2)) the
+// Legendre expansion above; elsewhere K and E from a fixed six-step float AGM
+// (converged for p >= 1e-3) -- the radial formula's cancellation there costs
+// at most ~eps_f / x of the ring's field scale.  Returns false (the caller
+// evaluates the pair in float64) when p = d2 / D < 1e-3: the point is close
+// to the ring itself.
 __device__ __forceinline__ bool ring_far_f(float rho, float inv_rho, float dr, float sr, float z, float a, float& er,
                                            float& ez) {
     const float z2 = z * z, a2 = a * a, rho2 = rho * rho;
+    if (rho2 < 0.09f * (a2 + z2)) {
+        ring_axis_f(rho, z, a, er, ez);
+        return true;
+    }
     const float D = fmaf(sr, sr, z2);
     const float d2 = fmaf(dr, dr, z2);
     const float invD = __frcp_rn(D);
     const float p = d2 * invD;
-    const bool ok = (p >= 1e-3f) && (rho2 >= 1e-4f * (a2 + z2));
+    const bool ok = p >= 1e-3f;
     const float pc = fmaxf(p, 1e-3f);
     float aa = 1.0f, bb = pc * rsqrtf(pc);
     float S = 0.5f * (1.0f - pc), w = 0.5f;

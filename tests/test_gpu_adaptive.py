@@ -81,6 +81,28 @@ def _tip_points(n, seed):
     return g, pts
 
 
+def test_bem_field_mixed_near_axis_benchmark_tip():
+    """Mixed form on the benchmark tip at points near the axis (where the
+    float32 Legendre branch takes almost every ring) from 2 nm to 1 mm above
+    the apex: within 1e-6 of the float64 reference rule, relative to the whole
+    field (uniform 1e6 V/m plus perturbation)."""
+    g = load_golden("sigma_c1")
+    prof, sig = g["profile"], g["sigma"]
+    apex = prof[:, 1].max()
+    rng = np.random.default_rng(12)
+    d = 10 ** rng.uniform(np.log10(2e-9), -3, 256)
+    rho = d * 10 ** rng.uniform(-4, -0.5, 256)
+    ph = rng.uniform(0, 2 * np.pi, 256)
+    pts = np.stack([rho * np.cos(ph), rho * np.sin(ph), apex + d], -1)
+    tab = BemTables(prof, sig, 8)
+    ref = engine.bem_field(tab, pts).cpu().numpy()
+    tot = np.linalg.norm(ref + np.array([0.0, 0.0, float(g["E_gun"])]), axis=-1)
+    for rule in ("reference", "adaptive"):
+        mix = engine.bem_field(tab, pts, form="mixed", far_rule=rule).cpu().numpy()
+        err = np.abs(mix - ref).max(axis=-1) / tot
+        assert err.max() < 1e-6, (rule, err.max())
+
+
 def test_run_bounds_leave_reference_rule_results_unchanged():
     """The closest-segment search and the near test skip runs of segments by
     their bounds; with the reference rule the field is bit-identical to the
