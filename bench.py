@@ -3,6 +3,14 @@ tracer's hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                     [--workload c1|c0|c2|c3|c4] [--attempts A] [--form fp64|mixed]
+                    [--far-rule reference|adaptive]
+
+The chosen form (the default): float32 + Kahan BEM and pair sums (float64
+state, stage combination, error norm and controller, float64 for points
+close to a ring) with the adaptive far-field rule.  The plain form (float64,
+the reference's quadrature) is timed in the same run on the same workload
+(`plain_fp64`), and `accuracy` reports the chosen form's endpoint error
+against it on a sample of groups traced to a fixed time.
 
 Workload (default c1, the largest single-GPU configuration with a BEM
 field): hemisphere R = 50 nm on a 5 um post, E = -1e6 V/m, 2000-panel BEM
@@ -155,7 +163,8 @@ def cpu_leg(name, n_procs, attempts, groups):
 def prepare_cpu_blob(name, wl):
     spec = wl["geometry"].spec()
     d = {k: v for k, v in wl["data"].items()}
-    blob = dict(spec=spec, data=d, rtol=wl["rtol"], atol=wl["atol"], t_max=wl["t_max"], z_max=wl["z_max"])
+    blob = dict(spec=spec, data=d, rtol=wl["rtol"], atol=wl["atol"], t_max=wl["t_max"], z_max=wl["z_max"],
+                config=wl["config"])
     import tempfile
     path = os.path.join(tempfile.gettempdir(), f"spt_bench_cpu_{name}_{os.getpid()}.npz")
     np.savez(path, wl=np.array(blob, dtype=object))
@@ -164,14 +173,17 @@ def prepare_cpu_blob(name, wl):
 
 
 def physical_cores():
+    """Worker processes for the CPU legs: the physical cores, at most 64, and
+    no more than the available host memory allows at ~1 GiB per worker (a
+    worker's float64 ring-sum temporaries over 64,000 nodes)."""
+    n = os.cpu_count() or 1
     try:
         import psutil
-        n = psutil.cpu_count(logical=False)
-        if n:
-            return n
+        n = psutil.cpu_count(logical=False) or n
+        n = min(n, max(1, int(psutil.virtual_memory().available / 2**30) // 2))
     except Exception:
         pass
-    return os.cpu_count() or 1
+    return max(1, min(n, 64))
 
 
 # ---------------------------------------------------------------------------
@@ -251,6 +263,29 @@ def fp64_peak_tflops(torch, dev):
     return 2.0 * n**3 / best / 1e12
 
 
+def fp32_peak_tflops(torch, dev, n=8192):
+    """Float32 CUDA-core peak measured in-run: a float32 GEMM with TF32 off."""
+    old = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        a = torch.randn(n, n, dtype=torch.float32, device=dev)
+        b = torch.randn(n, n, dtype=torch.float32, device=dev)
+        torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 1e30
+        for _ in range(5):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            torch.matmul(a, b)
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e) * 1e-3)
+        del a, b
+        return 2.0 * n**3 / best / 1e12
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = old
+
+
 def run_gpu(args, rank, world):
     import torch
     from bem_b200 import engine
@@ -307,11 +342,78 @@ def run_gpu(args, rank, world):
     if rank == 0 and not args.no_e2e:
         e2e = e2e_leg(args, wl, tracer, pos, vel, tb, q, m, cm, sizes, dev)
 
-    fp64_peak = fp64_peak_tflops(torch, dev) if rank == 0 else None
+    plain = None
+    acc = None
+    if rank == 0 and not args.no_plain and (args.form, args.far_rule) != ("fp64", "reference"):
+        plain = plain_leg(args, wl, pos, vel, tb, q, m, cm, sizes, dev)
+    if rank == 0 and not args.no_accuracy and (args.form, args.far_rule) != ("fp64", "reference"):
+        acc = accuracy_leg(args, wl, pos, vel, tb, q, m, cm, sizes, dev)
+    peak = (fp64_peak_tflops if args.form == "fp64" else fp32_peak_tflops)(torch, dev) if rank == 0 else None
     flops = dc["ring_far"] * FLOP_PER_RING + dc["ring_near"] * FLOP_PER_RING + dc["pair_evals"] * FLOP_PER_PAIR
     achieved = flops / t_total / 1e12
     return dict(value=steps_all / t_max_ranks, t_total=t_max_ranks, times=times, counters=dc, clocks=clk.summary(),
-                e2e=e2e, fp64_peak=fp64_peak, achieved=achieved, config=wl["config"], wl=wl)
+                e2e=e2e, peak=peak, achieved=achieved, config=wl["config"], wl=wl, plain=plain, accuracy=acc)
+
+
+def plain_leg(args, wl, pos, vel, tb, q, m, cm, sizes, dev):
+    """The plain form (float64, the reference's far quadrature) on the same
+    workload: the same W warm-up and K timed steps, CUDA events."""
+    import torch
+    from bem_b200 import engine
+
+    tracer = engine.Tracer(wl["geometry"], device=dev, form="fp64", z_max=wl["z_max"], far_rule="reference")
+    batch = engine.GroupBatch(pos, vel, tb, q, m, sizes, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    prm = lambda: tracer.params(wl["t_max"], wl["rtol"], wl["atol"], 1e-12, cm, args.attempts)
+    for _ in range(args.warmup):
+        tracer.launch(batch, prm(), stream)
+    torch.cuda.synchronize()
+    c0 = tracer.counter_dict()
+    t = 0.0
+    for _ in range(args.steps):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        tracer.launch(batch, prm(), stream)
+        e.record(stream)
+        e.synchronize()
+        t += s.elapsed_time(e) * 1e-3
+    steps = tracer.counter_dict()["particle_steps"] - c0["particle_steps"]
+    return dict(value=steps / t, unit=UNIT, ms_per_step=1e3 * t / args.steps, form="fp64", far_rule="reference")
+
+
+def accuracy_leg(args, wl, pos, vel, tb, q, m, cm, sizes, dev):
+    """Endpoint error of the chosen form against the plain form: the first
+    `acc_groups` groups traced to t_end = acc_time by both (a fixed end time,
+    so no endpoint depends on which step crossed z_max).  Particles alive at
+    t_end: |dx| / |x| and |dv| / |v| of the plain endpoint.  Particles that
+    returned to the emitter keep the state of the step that landed inside it,
+    which moves with the step sequence: they are compared by death time."""
+    import torch
+    from bem_b200 import engine
+
+    n = min(args.acc_groups, len(sizes))
+    k = int(np.sum(sizes[:n]))
+    out = {}
+    for form, rule in (("fp64", "reference"), (args.form, args.far_rule)):
+        tracer = engine.Tracer(wl["geometry"], device=dev, form=form, z_max=wl["z_max"], far_rule=rule)
+        batch = engine.GroupBatch(pos[:k], vel[:k], tb[:k], q[:k], m[:k], sizes[:n], device=dev)
+        tracer.run(batch, args.acc_time, wl["rtol"], wl["atol"], 1e-12, cm)
+        torch.cuda.synchronize()
+        c = tracer.counter_dict()
+        out[form, rule] = (batch.positions().cpu().numpy(), batch.velocities().cpu().numpy(),
+                           batch.t_death.cpu().numpy(), c["attempts"], c["accepted"])
+    (p0, v0, d0, a0, s0), (p1, v1, d1, a1, s1) = out[("fp64", "reference")], out[(args.form, args.far_rule)]
+    alive = ~np.isfinite(d0) & ~np.isfinite(d1)
+    dead = np.isfinite(d0) & np.isfinite(d1)
+    ex = np.linalg.norm(p1 - p0, axis=-1)[alive] / np.linalg.norm(p0, axis=-1)[alive]
+    ev = np.linalg.norm(v1 - v0, axis=-1)[alive] / np.linalg.norm(v0, axis=-1)[alive]
+    et = np.abs(d1[dead] - d0[dead]) / d0[dead]
+    return dict(groups=n, particles=k, t_end=args.acc_time, against="plain fp64 (reference quadrature) on the GPU",
+                alive=int(alive.sum()), max_rel_pos=float(ex.max()), median_rel_pos=float(np.median(ex)),
+                max_rel_vel=float(ev.max()), median_rel_vel=float(np.median(ev)),
+                killed=int(dead.sum()), killed_in_one_only=int((np.isfinite(d0) != np.isfinite(d1)).sum()),
+                max_rel_t_death=float(et.max()) if et.size else None,
+                attempts_plain=int(a0), attempts_chosen=int(a1), accepted_steps_ratio=float(s1 / s0))
 
 
 def e2e_leg(args, wl, tracer, pos, vel, tb, q, m, cm, sizes, dev):
@@ -349,11 +451,14 @@ def e2e_leg(args, wl, tracer, pos, vel, tb, q, m, cm, sizes, dev):
     return dict(value=steps / wall, unit=UNIT, h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(h2d))
 
 
-def load_traffic(workload, form):
-    path = os.path.join(REPO, "profiles", f"trace_kernel_{workload}_{form}.json")
-    if os.path.exists(path):
-        with open(path) as f:
-            return json.load(f)
+def load_traffic(workload, form, far_rule):
+    """DRAM bytes per trace launch from the committed ncu summary of this
+    workload and form (profiles/), or None."""
+    for name in (f"trace_kernel_{workload}_{form}_{far_rule}.json", f"trace_kernel_{workload}_{form}.json"):
+        path = os.path.join(REPO, "profiles", name)
+        if os.path.exists(path) and (far_rule == "reference" or name.endswith(f"_{far_rule}.json")):
+            with open(path) as f:
+                return json.load(f)
     return None
 
 
@@ -365,11 +470,15 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2", "c3", "c4"])
     ap.add_argument("--attempts", type=int, default=16, help="RK45 attempts per group per step")
-    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--far-rule", default="reference", choices=["reference", "adaptive"],
+    ap.add_argument("--form", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--far-rule", default="adaptive", choices=["reference", "adaptive"],
                     help="far-field quadrature of the BEM sum (adaptive: whole-segment Gauss-4/2 when distant)")
     ap.add_argument("--cpu-attempts", type=int, default=16)
     ap.add_argument("--groups", type=int, default=None, help="first N emission groups only (profiling a smaller case)")
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain form beside the chosen one")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the endpoint-error leg")
+    ap.add_argument("--acc-groups", type=int, default=64)
+    ap.add_argument("--acc-time", type=float, default=20e-12, help="end time of the endpoint-error traces [s]")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -395,20 +504,29 @@ def main():
         torch.distributed.destroy_process_group()
     if rank != 0:
         return 0
-    t = load_traffic(args.workload, args.form)
+    t = load_traffic(args.workload, args.form, args.far_rule)
     mean_ms = 1e3 * r["t_total"] / args.steps
+    fp64 = args.form == "fp64"
+    plain = r["plain"]
+    if plain is not None:
+        plain = dict(plain, ratio=r["value"] / plain["value"])
     line = dict(
         metric=METRIC, value=r["value"], unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
         ms_per_step=mean_ms, higher_is_better=True, scaling="weak", vs_baseline=None,
-        dtype="f64" if args.form == "fp64" else "f32+f64", data="synthetic (seeded samplers, workloads.py)",
-        config=dict(r["config"], form=args.form, far_rule=args.far_rule, attempts_per_step=args.attempts, parallelism=f"groups x {world} GPUs",
+        dtype="f64" if fp64 else "f32+f64", data="synthetic (seeded samplers, workloads.py)",
+        config=dict(r["config"], form=args.form, far_rule=args.far_rule, attempts_per_step=args.attempts,
+                    parallelism=f"groups x {world} GPUs",
                     l2="flushed between steps (256 MiB write); each step timed alone with CUDA events"),
         clocks=r["clocks"], gpu_launches=args.steps,
-        roofline=dict(bound="fp64", achieved=r["achieved"], peak=r["fp64_peak"], unit="TFLOP/s",
-                      frac=(r["achieved"] / r["fp64_peak"]) if r["fp64_peak"] else None,
+        roofline=dict(bound="fp64" if fp64 else "fp32", achieved=r["achieved"], peak=r["peak"], unit="TFLOP/s",
+                      frac=(r["achieved"] / r["peak"]) if r["peak"] else None,
                       traffic=(t or {}).get("dram_bytes_per_launch"),
-                      peak_source="measured in-run cuBLAS DGEMM (no FP64 figure in the driver's peak file)",
-                      flop_model=f"{FLOP_PER_RING:g} FLOP/ring eval, {FLOP_PER_PAIR:g} FLOP/pair"),
+                      peak_source=("measured in-run: cuBLAS DGEMM 4096^3" if fp64 else
+                                   "measured in-run: cuBLAS SGEMM 8192^3, TF32 off")
+                      + " (the driver's peak file has HBM and BF16 figures only)",
+                      flop_model=f"{FLOP_PER_RING:g} FLOP/ring eval, {FLOP_PER_PAIR:g} FLOP/pair (nominal)"),
+        plain_fp64=plain,
+        accuracy=r["accuracy"],
         counters=r["counters"],
         e2e=r["e2e"],
         cpu_baseline=cpu,
@@ -449,14 +567,30 @@ def _make_blob(name):
 
 
 def reference_arm(args, rank, world):
+    """The reference's algorithm for this path on the host cores (the NumPy
+    oracle port, float64, the reference's quadrature), on the same workload:
+    each step is a bounded sample -- one group per process, --cpu-attempts
+    attempts from emission.  Under torchrun only rank 0 runs."""
     if rank != 0:
         return 0
-    cpu = cpu_baseline(args)
-    line = dict(metric=METRIC, value=cpu["value"], unit=UNIT, n_gpus=world, steps=1, warmup=0,
-                ms_per_step=None, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f64",
-                data="synthetic (seeded samplers, workloads.py)", impl="reference",
-                config=dict(workload=args.workload, attempts_per_group=args.cpu_attempts),
-                cpu_baseline=cpu, e2e=dict(value=cpu["value"], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    wl = build_workload_cpu_side(args.workload)
+    procs = min(physical_cores(), 64)
+    groups = list(range(min(procs, len(wl["data"]["group_sizes"]))))
+    total_steps, total_wall = 0, 0.0
+    for _ in range(args.steps):
+        value, steps, wall, _ = cpu_leg(args.workload, procs, args.cpu_attempts, groups)
+        total_steps += steps
+        total_wall += wall
+    value = total_steps / total_wall
+    cpu = dict(value=value, unit=UNIT, cores=procs, kind="port",
+               sample=f"per step {len(groups)} groups x {args.cpu_attempts} attempts from emission, one group per "
+                      f"process; {args.steps} steps, {total_steps} accepted particle-steps in {total_wall:.1f} s")
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=0,
+                ms_per_step=1e3 * total_wall / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f64", data="synthetic (seeded samplers, workloads.py)", impl="reference",
+                config=dict(wl.get("config", {}), form="fp64 (reference algorithm, NumPy port)",
+                            attempts_per_step=args.cpu_attempts),
+                cpu_baseline=cpu, e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line))
     return 0
 
