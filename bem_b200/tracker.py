@@ -70,7 +70,7 @@ def group_indices(particle_group, n_emit):
 class SpecificParticleTracer:
     def __init__(self, initial_particles, n_emit, geometry, screens, t_out=None,
                  plummer_radius=DEFAULT_PLUMMER_RADIUS, backend="b200", n_workers=1, rtol=None, atol=None,
-                 t_max=None, z_max=None, form="fp64", device="cuda"):
+                 t_max=None, z_max=None, form="fp64", device="cuda", far_rule="reference"):
         if n_workers != 1:
             raise ValueError(
                 f"n_workers is only supported for backend='cpu' (got backend={backend!r}, n_workers={n_workers!r})")
@@ -93,6 +93,7 @@ class SpecificParticleTracer:
         self.rtol = rtol if rtol is not None else DEFAULT_RTOL
         self.atol = atol if atol is not None else DEFAULT_ATOL
         self.form = form
+        self.far_rule = far_rule
         self.device = device
         self._setup_state()
         self.t_max = t_max if t_max is not None else self._default_t_max()
@@ -139,7 +140,8 @@ class SpecificParticleTracer:
 
     def run(self, verbose=False):
         """tracker.py:312-386 -> (screen ParticleGroups, trajectory ParticleGroups)."""
-        tracer = engine.Tracer(self.geometry, device=self.device, form=self.form, z_max=self.z_max)
+        tracer = engine.Tracer(self.geometry, device=self.device, form=self.form, z_max=self.z_max,
+                               far_rule=self.far_rule)
         batch = engine.GroupBatch(self.pos0, self.vel0, self.t_birth, self.charge, self.particle_mass,
                                   [self.n_per_group] * self.n_groups, device=self.device)
         rec = tracer.run(batch, self.t_max, self.rtol, self.atol, self.plummer_radius, self.charge_to_mass,
