@@ -49,7 +49,7 @@ class SptState(ctypes.Structure):
                 ("group_offset", _p), ("group_order", _p),
                 ("x", _p), ("y", _p), ("z", _p), ("vx", _p), ("vy", _p), ("vz", _p),
                 ("t_birth", _p), ("t_death", _p), ("charge", _p), ("mass", _p),
-                ("t", _p), ("h", _p), ("status", _p), ("n_accepted", _p), ("n_rejected", _p)]
+                ("t", _p), ("h", _p), ("status", _p), ("n_accepted", _p), ("n_rejected", _p), ("n_active", _p)]
 
 
 class SptTraceParams(ctypes.Structure):
@@ -95,6 +95,7 @@ SIGNATURES = {
     "spt_bem_field": (ctypes.c_int, [_p, _p, _p, _i64, ctypes.POINTER(SptBem), _i32, _p, _p, _p, _p]),
     "spt_surrogate_field": (ctypes.c_int, [_p, _p, _p, _i64, ctypes.POINTER(SptBem), ctypes.POINTER(SptTraceParams),
                                            _p, _p, _p, _p]),
+    "spt_compact_groups": (ctypes.c_int, [_p, _i32, _p, _p, _p, _p]),
     "spt_ring_field": (ctypes.c_int, [_p, _p, _p, _i64, _i32, _p, _p, _p]),
     "spt_ellip_ke": (ctypes.c_int, [_p, _i64, _i32, _p, _p, _p]),
     "spt_bem_assemble": (ctypes.c_int, [_p, _p, _i32, _d, _i32, _p, _p, _p, _p]),

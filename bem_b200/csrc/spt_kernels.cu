@@ -1615,12 +1615,14 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
     if (sur) bind_surrogate(c, prm, &s_tmem);
     init_barriers(c);
 
+    // groups to process: all, or the compacted running ones (count written on the device)
+    const int n_run = st.n_active ? *st.n_active : st.n_groups;
     for (;;) {
         if (tid == 0) s_g = atomicAdd(work, 1);
         __syncthreads();
         const int gi = s_g;
         __syncthreads();
-        if (gi >= st.n_groups) break;
+        if (gi >= n_run) break;
         const int g = st.group_order ? st.group_order[gi] : gi;
         const long long base = st.group_offset[g];
         const int E = (int)(st.group_offset[g + 1] - base);
@@ -1955,6 +1957,39 @@ surrogate_field_kernel(const double* x, const double* y, const double* z, long l
     release_surrogate(c);
 }
 
+// order-preserving compaction of the running groups (spt_compact_groups):
+// one CTA of kCompactThreads walks the list in chunks; each chunk is read,
+// scanned (warp ballots + per-warp counts) and written after a barrier, so
+// out may alias order (a chunk's writes land at or before its reads).
+constexpr int kCompactThreads = 1024;
+__global__ void __launch_bounds__(kCompactThreads, 1)
+compact_kernel(const int* order, int n, const int* status, int* out, int* n_active) {
+    __shared__ int s_w[kCompactThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int run = 0;
+    for (int base = 0; base < n; base += kCompactThreads) {
+        const int j = base + tid;
+        int g = 0;
+        bool keep = false;
+        if (j < n) {
+            g = order ? order[j] : j;
+            keep = status[g] < SPT_GROUP_DONE;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_w[warp] = __popc(bal);
+        __syncthreads();
+        int pre = 0, tot = 0;
+        for (int w = 0; w < kCompactThreads / 32; ++w) {
+            if (w < warp) pre += s_w[w];
+            tot += s_w[w];
+        }
+        if (keep) out[run + pre + __popc(bal & ((1u << lane) - 1u))] = g;
+        run += tot;
+        __syncthreads();
+    }
+    if (tid == 0) *n_active = run;
+}
+
 __global__ void ring_kernel(const double* rho, const double* z, const double* a, long long n, int form, double* er,
                             double* ez) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
@@ -2182,6 +2217,7 @@ int spt_trace(const SptState* s, const SptTraceParams* p, const SptGeometry* g, 
     if (s->n_groups <= 0) return SPT_OK;
     if (s->max_group_size <= 0 || s->max_group_size > 1024)
         return fail(SPT_ERR_CAPACITY, "max_group_size %d outside [1, 1024]", s->max_group_size);
+    if (s->n_active && !s->group_order) return fail(SPT_ERR_ARG, "n_active needs group_order");
     if (reinterpret_cast<uintptr_t>(ws) & 255) return fail(SPT_ERR_ARG, "workspace must be 256-byte aligned");
     if (p->form != SPT_FORM_FP64 && p->form != SPT_FORM_MIXED && p->form != SPT_FORM_SURROGATE)
         return fail(SPT_ERR_ARG, "unknown form %d", p->form);
@@ -2269,6 +2305,13 @@ int spt_surrogate_field(const double* x, const double* y, const double* z, int64
     spt::surrogate_field_kernel<<<(unsigned)blocks, spt::kThreads, L.bytes, static_cast<cudaStream_t>(stream)>>>(
         x, y, z, n, *b, *sur, ex, ey, ez, nullptr);
     return cuda_check(cudaGetLastError(), "surrogate_field_kernel launch");
+}
+
+int spt_compact_groups(const int32_t* order, int32_t n, const int32_t* status, int32_t* out, int32_t* n_active,
+                       void* stream) {
+    if (!status || !out || !n_active || n < 0) return fail(SPT_ERR_ARG, "null argument");
+    spt::compact_kernel<<<1, spt::kCompactThreads, 0, static_cast<cudaStream_t>(stream)>>>(order, n, status, out, n_active);
+    return cuda_check(cudaGetLastError(), "compact_kernel launch");
 }
 
 int spt_ring_field(const double* rho, const double* z, const double* a, int64_t n, int32_t form, double* er,
@@ -2376,6 +2419,7 @@ extern "C" int spt_trace_noalloc(const SptState* s, const SptTraceParams* p, con
     if (s->n_groups <= 0) return SPT_OK;
     if (s->max_group_size <= 0 || s->max_group_size > 1024)
         return fail(SPT_ERR_CAPACITY, "spt_trace_noalloc: max_group_size %d outside [1, 1024]", s->max_group_size);
+    if (s->n_active && !s->group_order) return fail(SPT_ERR_ARG, "n_active needs group_order");
     if (p->form != SPT_FORM_FP64 && p->form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "unknown form %d", p->form);
     if (p->form == SPT_FORM_SURROGATE) return fail(SPT_ERR_ARG, "spt_trace_noalloc: the learned form is not offered");
     if (is_bem(g->kind)) {

@@ -68,6 +68,8 @@ class GroupBatch:
         self.t_birth = _as_dev(t_birth, f64, d).reshape(-1)
         self.charge = _as_dev(charge, f64, d).reshape(-1)
         self.mass = _as_dev(mass, f64, d).reshape(-1)
+        self.live = None       # compacted processing order (enable_compaction)
+        self.n_active = None
         self.t_death = torch.full((n,), float("inf"), dtype=f64, device=d)
         G = self.n_groups
         self.t = torch.zeros(G, dtype=f64, device=d)
@@ -75,6 +77,27 @@ class GroupBatch:
         self.status = torch.zeros(G, dtype=torch.int32, device=d)
         self.n_accepted = torch.zeros(G, dtype=torch.int64, device=d)
         self.n_rejected = torch.zeros(G, dtype=torch.int64, device=d)
+
+    def enable_compaction(self):
+        """Process only the running groups: `compact()` (on the device, no
+        host sync) rebuilds the processing order from the statuses."""
+        torch = _torch()
+        if self.live is None:
+            base = self.order if self.order is not None else torch.arange(self.n_groups, dtype=torch.int32,
+                                                                          device=self.device)
+            self.live = base.clone()
+            self.n_active = torch.full((1,), self.n_groups, dtype=torch.int32, device=self.device)
+
+    def compact(self, stream=None):
+        """spt_compact_groups on `stream`: live = the running groups of the
+        processing order, n_active = their number."""
+        torch = _torch()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        base = self.order.data_ptr() if self.order is not None else None
+        _lib.check(_lib.lib().spt_compact_groups(base, self.n_groups, self.status.data_ptr(), self.live.data_ptr(),
+                                                 self.n_active.data_ptr(), ctypes.c_void_p(stream.cuda_stream)),
+                   "spt_compact_groups")
 
     def struct(self):
         s = _lib.SptState()
@@ -84,6 +107,9 @@ class GroupBatch:
         P = lambda t: None if t is None else t.data_ptr()
         s.group_offset = P(self.offsets)
         s.group_order = P(self.order)
+        if self.live is not None:
+            s.group_order = P(self.live)
+            s.n_active = P(self.n_active)
         s.x, s.y, s.z = P(self.x), P(self.y), P(self.z)
         s.vx, s.vy, s.vz = P(self.vx), P(self.vy), P(self.vz)
         s.t_birth, s.t_death = P(self.t_birth), P(self.t_death)
@@ -188,14 +214,27 @@ class Tracer:
 
     def run(self, batch, t_max, rtol, atol, plummer_radius, charge_to_mass, max_steps=10_000_000,
             attempt_chunk=DEFAULT_ATTEMPT_CHUNK, log_capacity=0, screens=None, output_times=None,
-            screen_capacity=None, **kw):
+            screen_capacity=None, compact=False, graph=False, graph_launches=4, **kw):
         """Integrate every group to t_max.  Raises RuntimeError when a group
         needs more than max_steps attempts (batched_rk45.py:320-321).
 
         With `screens` (z planes) and/or `output_times`, returns a
         TraceRecords holding every crossing and every output-time snapshot;
-        otherwise returns the attempt log (or None)."""
+        otherwise returns the attempt log (or None).
+
+        compact: before every launch, retired groups are dropped from the
+        processing order on the device (spt_compact_groups).  graph (implies
+        compact): `graph_launches` x [compact, spt_trace of attempt_chunk
+        attempts] are captured once as a CUDA graph and replayed, the host
+        checking the statuses once per replay."""
         torch = _torch()
+        if graph:
+            if screens or output_times is not None or log_capacity:
+                raise ValueError("graph=True records neither screens, output times nor attempt logs")
+            return self._run_graph(batch, t_max, rtol, atol, plummer_radius, charge_to_mass, max_steps,
+                                   attempt_chunk, graph_launches, **kw)
+        if compact:
+            batch.enable_compaction()
         records = None
         if screens or output_times is not None:
             records = TraceRecords(batch, screens or [], output_times, self.device, screen_capacity)
@@ -210,19 +249,58 @@ class Tracer:
             if chunk <= 0:
                 raise RuntimeError(f"batched RK45 did not converge within {max_steps} steps")
             p = self.params(t_max, rtol, atol, plummer_radius, charge_to_mass, chunk, log=log, **kw)
+            if compact:
+                batch.compact()
             self.launch(batch, p)
             done_attempts += chunk
             if records is not None:
                 records.collect()
-            status = batch.status.cpu().numpy()
-            bad = np.isin(status, [_lib.GROUP_NONFINITE, _lib.GROUP_TIMEOUT])
-            if np.any(bad):
-                g = int(np.nonzero(bad)[0][0])
-                raise RuntimeError(f"group {g} stopped with status {int(status[g])} "
-                                   f"({'non-finite error norm' if status[g] == _lib.GROUP_NONFINITE else 'device wait timeout'})")
-            if np.all(status == _lib.GROUP_DONE):
+            if self._check_done(batch):
                 break
         return records if records is not None else log
+
+    @staticmethod
+    def _check_done(batch):
+        status = batch.status.cpu().numpy()
+        bad = np.isin(status, [_lib.GROUP_NONFINITE, _lib.GROUP_TIMEOUT])
+        if np.any(bad):
+            g = int(np.nonzero(bad)[0][0])
+            raise RuntimeError(f"group {g} stopped with status {int(status[g])} "
+                               f"({'non-finite error norm' if status[g] == _lib.GROUP_NONFINITE else 'device wait timeout'})")
+        return bool(np.all(status == _lib.GROUP_DONE))
+
+    def _run_graph(self, batch, t_max, rtol, atol, plummer_radius, charge_to_mass, max_steps, attempt_chunk,
+                   graph_launches, **kw):
+        torch = _torch()
+        batch.enable_compaction()
+        chunk = min(attempt_chunk, max_steps)
+        p = self.params(t_max, rtol, atol, plummer_radius, charge_to_mass, chunk, **kw)
+        # one eager chunk first: sizes the workspace and sets the kernel attributes outside the capture
+        batch.compact()
+        self.launch(batch, p)
+        done_attempts = chunk
+        if self._check_done(batch):
+            return None
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, capture_error_mode="thread_local"):
+            for _ in range(graph_launches):
+                batch.compact()
+                self.launch(batch, p)
+        self._graph = g  # kept alive with its parameter blocks
+        while True:
+            if done_attempts + graph_launches * chunk <= max_steps:
+                g.replay()
+                done_attempts += graph_launches * chunk
+            else:
+                # the last attempts before max_steps: eager launches, never past it
+                rest = min(chunk, max_steps - done_attempts)
+                if rest <= 0:
+                    raise RuntimeError(f"batched RK45 did not converge within {max_steps} steps")
+                batch.compact()
+                self.launch(batch, self.params(t_max, rtol, atol, plummer_radius, charge_to_mass, rest, **kw))
+                done_attempts += rest
+            if self._check_done(batch):
+                return None
 
     def counter_dict(self):
         c = self.counters.cpu().numpy().astype(np.uint64)

@@ -174,6 +174,11 @@ typedef struct {
     int32_t* status;               /* [n_groups] SPT_GROUP_* */
     int64_t* n_accepted;           /* [n_groups] */
     int64_t* n_rejected;           /* [n_groups] */
+    /* Optional device count: process only group_order[0, *n_active) (the
+     * running groups after spt_compact_groups; lets a captured CUDA graph
+     * shrink its work without host involvement).  NULL: all n_groups.
+     * Needs group_order. */
+    const int32_t* n_active;
 } SptState;
 
 typedef struct {
@@ -262,6 +267,14 @@ typedef struct {
     double* ax; double* ay; double* az;
 } SptAccelArgs;
 int spt_accel(const SptAccelArgs* args, const SptGeometry* geom, const SptBem* bem, void* stream);
+
+/* Compaction of retired groups: out[0, *n_active) = the entries g of
+ * order[0, n) (the identity when order is NULL) with status[g] <
+ * SPT_GROUP_DONE, in order.  out may alias order.  One CTA; no host sync,
+ * so it can be captured in a CUDA graph with the spt_trace calls that
+ * follow it. */
+int spt_compact_groups(const int32_t* order, int32_t n, const int32_t* status, int32_t* out, int32_t* n_active,
+                       void* stream);
 
 /* Perturbation field E = -grad S[sigma] of the BEM solution at n points
  * (x, y, z) -> (ex, ey, ez), all [n] device arrays. */
