@@ -61,7 +61,7 @@ class SptTraceParams(ctypes.Structure):
                 ("screen_capacity", _i64), ("screen_count", _p), ("output_times", _p), ("output_rec", _p),
                 ("output_flag", _p), ("sur_w", _p), ("sur_w16", _p), ("sur_s_start", _p), ("sur_log_scale", _p),
                 ("sur_s_end", _d), ("sur_sig_floor", _d), ("sur_band", _d), ("sur_spot", _d), ("sur_d_min", _d),
-                ("sur_d_max", _d), ("sur_stats", _p)]
+                ("sur_d_max", _d), ("sur_stats", _p), ("round_points", _i32), ("reserved2", _i32)]
 
 
 class SptAccelArgs(ctypes.Structure):

@@ -1,0 +1,165 @@
+"""Autotuner for the trace's launch configuration.
+
+The knobs change speed, not physics:
+
+* ``round_points`` -- the far-sum tile shape: evaluation points per round
+  (1, 2, 4, 8).  Fewer points give each thread more nodes in flight per
+  point; more points share node loads and the adaptive rule's
+  classification.  Results agree to rounding.
+* ``ratios`` -- thresholds (ratio4, ratio2, ratio_run) of the adaptive far
+  rule.  Candidates pass an accuracy guard first: at the sample's own
+  trajectory points their float64 field must match the reference quadrature
+  to ``tol`` of the whole field (uniform plus perturbation); a candidate that
+  does not is never timed.
+* ``order`` -- group processing order ("largest_first" or "given").
+
+Procedure: a sample of groups (every k-th group, so that every size range is
+represented) is advanced `warm` attempts from emission, the warmed state is
+saved, and each candidate runs `attempts` attempts from that state, timed
+with CUDA events (best of `repeats`).  Coordinate descent: round_points,
+then ratios, then order.  The winner is applied to a Tracer / GroupBatch with
+``apply``.  Results can be cached in a JSON file keyed by the geometry,
+form, rule and group-size mix.
+"""
+
+import json
+import os
+
+import numpy as np
+
+from . import _lib, engine, tables
+
+ROUND_POINTS = (8, 4, 2)
+RATIOS = ((tables.RATIO4, tables.RATIO2, tables.RATIO_RUN), (6.0, 150.0, 3.0), (12.0, 600.0, 6.0),
+          (16.0, 1000.0, 8.0))
+ORDERS = ("largest_first", "given")
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def signature(tracer, sizes):
+    """Cache key: geometry kind and panel count, form, rule, size mix."""
+    sizes = np.asarray(sizes)
+    hist = np.histogram(np.log2(np.maximum(sizes, 1)), bins=[0, 2, 4, 6, 8, 11])[0]
+    n_seg = tracer.tables.n_seg if tracer.tables is not None else 0
+    frac = tuple(int(round(100 * h / len(sizes))) for h in hist)
+    return f"kind{tracer.geom.kind}-seg{n_seg}-form{tracer.form}-{tracer.far_rule}-sizes{frac}"
+
+
+class TuneResult(dict):
+    """config (round_points, ratios, order) plus the timings behind it."""
+
+
+def _sample(sizes, n_sample):
+    G = len(sizes)
+    if G <= n_sample:
+        return np.arange(G)
+    return np.linspace(0, G - 1, n_sample).round().astype(np.int64)
+
+
+def _accuracy_ok(tracer, pos, ratios, tol):
+    """Float64 field of the candidate adaptive rule against the reference
+    rule at the given points, relative to the whole field there."""
+    if tracer.tables is None or tracer.far_rule != "adaptive":
+        return True
+    geo = tracer.geometry
+    pts = pos[(pos[:, 2] >= 0.0) & np.isfinite(pos).all(axis=1)]
+    if len(pts) == 0:
+        return True
+    ref = engine.bem_field(tracer.tables, pts).cpu().numpy()
+    got = engine.bem_field(tracer.tables, pts, far_rule="adaptive", ratio4=ratios[0], ratio2=ratios[1],
+                           ratio_run=ratios[2]).cpu().numpy()
+    tot = np.linalg.norm(ref + np.array([0.0, 0.0, float(geo.E_gun)]), axis=-1)
+    return bool(np.all(np.abs(got - ref).max(axis=-1) <= tol * tot))
+
+
+def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plummer_radius, charge_to_mass,
+         n_sample=592, warm=24, attempts=8, repeats=2, tol=1e-11, cache=None):
+    """Choose round_points, the adaptive rule's ratios and the processing
+    order for `tracer` on this workload (arrays as for GroupBatch).  Returns a
+    TuneResult; `apply` sets it.  `cache`: a JSON file path (read if it holds
+    this signature, updated otherwise)."""
+    torch = _torch()
+    sizes = np.asarray(sizes, dtype=np.int64)
+    key = signature(tracer, sizes)
+    if cache and os.path.exists(cache):
+        with open(cache) as f:
+            stored = json.load(f)
+        if key in stored:
+            return TuneResult(stored[key], cached=True)
+    groups = _sample(sizes, n_sample)
+    offs = np.concatenate([[0], np.cumsum(sizes)])
+    rows = np.concatenate([np.arange(offs[g], offs[g + 1]) for g in groups])
+    sub = (np.asarray(pos)[rows], np.asarray(vel)[rows], np.asarray(t_birth)[rows], np.asarray(charge)[rows],
+           np.asarray(mass)[rows], sizes[groups])
+    base = engine.GroupBatch(*sub, device=tracer.device)
+    prm = lambda a, rp=None: tracer.params(t_max, rtol, atol, plummer_radius, charge_to_mass, a, round_points=rp)
+    tracer.launch(base, prm(warm))
+    torch.cuda.synchronize()
+    work = engine.GroupBatch(*sub, device=tracer.device)
+    saved_bem, saved_rp = tracer.bem, tracer.round_points
+
+    def timed(order, rp, ratios):
+        if tracer.tables is not None:
+            tracer.bem = tracer.tables.view(tracer.far_rule, ratio4=ratios[0], ratio2=ratios[1], ratio_run=ratios[2])
+        work.set_order(order)
+        best = float("inf")
+        steps = 0
+        for _ in range(repeats):
+            work.copy_state_from(base)
+            c0 = tracer.counter_dict()["particle_steps"]
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            tracer.launch(work, prm(attempts, rp))
+            e.record()
+            e.synchronize()
+            best = min(best, s.elapsed_time(e) * 1e-3)
+            steps = tracer.counter_dict()["particle_steps"] - c0
+        return steps / best
+
+    timings = {}
+    cfg = dict(round_points=8, ratios=list(RATIOS[0]), order="largest_first")
+    try:
+        rates = {}
+        for rp in ROUND_POINTS:
+            rates[rp] = timings[f"round_points={rp}"] = timed(cfg["order"], rp, cfg["ratios"])
+        cfg["round_points"] = max(rates, key=rates.get)
+        if tracer.tables is not None and tracer.far_rule == "adaptive":
+            sample_pos = base.positions().cpu().numpy()
+            rates = {}
+            for r in RATIOS:
+                if not _accuracy_ok(tracer, sample_pos, r, tol):
+                    timings[f"ratios={r}"] = "rejected by the accuracy guard"
+                    continue
+                rates[r] = timings[f"ratios={r}"] = timed(cfg["order"], cfg["round_points"], r)
+            cfg["ratios"] = list(max(rates, key=rates.get))
+        rates = {}
+        for o in ORDERS:
+            rates[o] = timings[f"order={o}"] = timed(o, cfg["round_points"], cfg["ratios"])
+        cfg["order"] = max(rates, key=rates.get)
+    finally:
+        tracer.bem, tracer.round_points = saved_bem, saved_rp
+    res = TuneResult(cfg, timings=timings, key=key, sample_groups=len(groups), attempts=attempts, warm=warm)
+    if cache:
+        stored = {}
+        if os.path.exists(cache):
+            with open(cache) as f:
+                stored = json.load(f)
+        stored[key] = dict(cfg)
+        with open(cache, "w") as f:
+            json.dump(stored, f, indent=1)
+    return res
+
+
+def apply(config, tracer, batch=None):
+    """Set a tuned configuration on a Tracer (and a GroupBatch's order)."""
+    tracer.round_points = int(config["round_points"])
+    if tracer.tables is not None:
+        r = config["ratios"]
+        tracer.bem = tracer.tables.view(tracer.far_rule, ratio4=r[0], ratio2=r[1], ratio_run=r[2])
+    if batch is not None:
+        batch.set_order(config["order"])
+    return tracer

@@ -256,6 +256,7 @@ struct Ctx {
     double kc;       // Coulomb constant 1/(4 pi eps0)
     double soft2;    // plummer^2
     int form;
+    int round_pts;           // points per far-sum round, 1..kRound
     int E;
     double* base;    // dynamic smem
     Layout L;
@@ -284,6 +285,7 @@ __device__ inline void bind(Ctx& c, double* smem, int E, double* slot, bool sur 
     c.base = smem;
     c.E = E;
     c.L = make_layout(E, true, sur);
+    c.round_pts = kRound;
     const Layout& L = c.L;
     if (!L.big) {
         c.y0 = smem + L.y0;
@@ -901,7 +903,7 @@ __device__ void bem_sums(Ctx& c, int n, int* status_flag) {
     if (lane == 0) { c.cnt[SPT_CNT_NEAR_PAIRS] += n_near; c.cnt[SPT_CNT_RING_NEAR] += n_ring_near; }
     __syncthreads();
 
-    // C: far sum, rounds of up to kRound points over TMA-staged node tiles;
+    // C: far sum, rounds of up to c.round_pts points over TMA-staged node tiles;
     // the round's point count selects how many nodes each thread keeps in
     // flight so that every thread has 8 independent ring evaluations.
     const int tile_cap = c.L.tile_cap;
@@ -909,8 +911,8 @@ __device__ void bem_sums(Ctx& c, int n, int* status_flag) {
     const int n_tiles = (nseg + segs_per_tile - 1) / segs_per_tile;
     unsigned long long far_evals = 0;
     bool ok = true;
-    for (int r0 = 0; r0 < n; r0 += kRound) {
-        const int np_ = min(kRound, n - r0);
+    for (int r0 = 0; r0 < n; r0 += c.round_pts) {
+        const int np_ = min(c.round_pts, n - r0);
         if (b.far_rule == SPT_FAR_ADAPTIVE) {
             const bool mix = c.form != SPT_FORM_FP64;
             if (np_ == 1) mix ? far_adaptive<1, 8, true>(c, r0, np_, far_evals) : far_adaptive<1, 8, false>(c, r0, np_, far_evals);
@@ -1608,6 +1610,7 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
     c.kc = prm.coulomb_constant;
     c.soft2 = prm.plummer_radius * prm.plummer_radius;
     c.form = prm.form;
+    c.round_pts = (prm.round_points >= 1 && prm.round_points <= kRound) ? prm.round_points : kRound;
     const int Emax = st.max_group_size;
     const bool sur = prm.form == SPT_FORM_SURROGATE;
     bind(c, smem, Emax, big_slots ? big_slots + (size_t)blockIdx.x * big_slot_doubles(Emax) : nullptr, sur);

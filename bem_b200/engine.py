@@ -78,6 +78,27 @@ class GroupBatch:
         self.n_accepted = torch.zeros(G, dtype=torch.int64, device=d)
         self.n_rejected = torch.zeros(G, dtype=torch.int64, device=d)
 
+    STATE = ("x", "y", "z", "vx", "vy", "vz", "t_death", "t", "h", "status", "n_accepted", "n_rejected")
+
+    def copy_state_from(self, other):
+        """Copy the evolving state (positions, velocities, deaths, group
+        clocks and counts) of a batch with the same groups."""
+        for k in self.STATE:
+            getattr(self, k).copy_(getattr(other, k))
+
+    def set_order(self, order):
+        """Processing order: "largest_first" or "given" (group index order)."""
+        torch = _torch()
+        if order == "largest_first":
+            perm = np.argsort(-self.sizes, kind="stable").astype(np.int32)
+            self.order = torch.as_tensor(perm, device=self.device)
+        elif order == "given":
+            self.order = None
+        else:
+            raise ValueError(order)
+        self.live = None
+        self.n_active = None
+
     def enable_compaction(self):
         """Process only the running groups: `compact()` (on the device, no
         host sync) rebuilds the processing order from the statuses."""
@@ -150,6 +171,7 @@ class Tracer:
         self.geom = geometry.to_struct(z_max=z_max)
         self.tables = geometry.bem_tables(self.device) if geometry.is_bem else None
         self.far_rule = far_rule
+        self.round_points = 0  # far-sum points per round (0: the kernel's default, 8); see autotune
         self.bem = None
         if self.tables is not None:
             kw = {k: v for k, v in (("ratio4", ratio4), ("ratio2", ratio2), ("ratio_run", ratio_run)) if v is not None}
@@ -164,8 +186,9 @@ class Tracer:
 
     def params(self, t_max, rtol, atol, plummer_radius, charge_to_mass, max_attempts, log=None,
                safety=0.9, min_factor=0.2, max_factor=10.0, initial_step_fraction=1e-6,
-               coulomb_constant=COULOMB_CONSTANT, records=None):
+               coulomb_constant=COULOMB_CONSTANT, records=None, round_points=None):
         p = _lib.SptTraceParams()
+        p.round_points = int(self.round_points if round_points is None else round_points)
         p.t_max, p.rtol, p.atol = float(t_max), float(rtol), float(atol)
         p.plummer_radius = float(plummer_radius)
         p.charge_to_mass = float(charge_to_mass)

@@ -300,6 +300,16 @@ def run_gpu(args, rank, world):
     sizes = wl["data"]["group_sizes"]
     tracer = engine.Tracer(wl["geometry"], device=dev, form=args.form, z_max=wl["z_max"], far_rule=args.far_rule)
     batch = engine.GroupBatch(pos, vel, tb, q, m, sizes, device=dev)
+    tuned = None
+    if args.tune:
+        # launch configuration chosen by the project's autotuner on a sample of this workload (untimed)
+        from bem_b200 import autotune
+        t0 = time.perf_counter()
+        res = autotune.tune(tracer, pos, vel, tb, q, m, sizes, wl["t_max"], wl["rtol"], wl["atol"], 1e-12, cm)
+        autotune.apply(res, tracer, batch)
+        tracer.tuned_order = res["order"]
+        tuned = dict(res, seconds=round(time.perf_counter() - t0, 2), sample_groups=res.get("sample_groups"),
+                     timings={k: (round(v) if isinstance(v, float) else v) for k, v in res.get("timings", {}).items()})
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     prm = lambda: tracer.params(wl["t_max"], wl["rtol"], wl["atol"], 1e-12, cm, args.attempts)
@@ -352,7 +362,8 @@ def run_gpu(args, rank, world):
     flops = dc["ring_far"] * FLOP_PER_RING + dc["ring_near"] * FLOP_PER_RING + dc["pair_evals"] * FLOP_PER_PAIR
     achieved = flops / t_total / 1e12
     return dict(value=steps_all / t_max_ranks, t_total=t_max_ranks, times=times, counters=dc, clocks=clk.summary(),
-                e2e=e2e, peak=peak, achieved=achieved, config=wl["config"], wl=wl, plain=plain, accuracy=acc)
+                e2e=e2e, peak=peak, achieved=achieved, config=wl["config"], wl=wl, plain=plain, accuracy=acc,
+                tuned=tuned)
 
 
 def plain_leg(args, wl, pos, vel, tb, q, m, cm, sizes, dev):
@@ -423,6 +434,8 @@ def e2e_leg(args, wl, tracer, pos, vel, tb, q, m, cm, sizes, dev):
     from bem_b200 import engine
 
     batch = engine.GroupBatch(pos, vel, tb, q, m, sizes, device=dev)
+    if getattr(tracer, "tuned_order", None):
+        batch.set_order(tracer.tuned_order)
     names = ["x", "y", "z", "vx", "vy", "vz", "t_death", "t", "h", "status", "n_accepted", "n_rejected"]
     host = {k: torch.empty_like(getattr(batch, k), device="cpu").pin_memory() for k in names}
     for k in names:
@@ -476,6 +489,7 @@ def main():
     ap.add_argument("--cpu-attempts", type=int, default=16)
     ap.add_argument("--groups", type=int, default=None, help="first N emission groups only (profiling a smaller case)")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain form beside the chosen one")
+    ap.add_argument("--tune", action="store_true", help="autotune the launch configuration first (untimed)")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the endpoint-error leg")
     ap.add_argument("--acc-groups", type=int, default=64)
     ap.add_argument("--acc-time", type=float, default=20e-12, help="end time of the endpoint-error traces [s]")
@@ -515,6 +529,7 @@ def main():
         ms_per_step=mean_ms, higher_is_better=True, scaling="weak", vs_baseline=None,
         dtype="f64" if fp64 else "f32+f64", data="synthetic (seeded samplers, workloads.py)",
         config=dict(r["config"], form=args.form, far_rule=args.far_rule, attempts_per_step=args.attempts,
+                    autotuned=r["tuned"],
                     parallelism=f"groups x {world} GPUs",
                     l2="flushed between steps (256 MiB write); each step timed alone with CUDA events"),
         clocks=r["clocks"], gpu_launches=args.steps,

@@ -231,6 +231,13 @@ typedef struct {
     const double* sur_log_scale;
     double sur_s_end, sur_sig_floor, sur_band, sur_spot, sur_d_min, sur_d_max;
     unsigned long long* sur_stats;
+    /* Far-sum tile shape: evaluation points per round, 1, 2, 4 or 8 (0 or
+     * anything else: 8).  Fewer points per round give each thread more
+     * nodes in flight per point; more points share each node load and each
+     * round's classification.  Results agree to rounding (and, with the
+     * adaptive rule, to its ~1e-14 classification effect). */
+    int32_t round_points;
+    int32_t reserved2;
 } SptTraceParams;
 
 /* Scratch bytes spt_trace needs for this state/geometry (work-queue

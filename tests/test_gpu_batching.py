@@ -80,3 +80,41 @@ def test_graph_run_respects_max_steps():
         tr.run(b, 3e-12, 1e-8, 1e-12, 1e-12, gu.CM, max_steps=200, attempt_chunk=64, graph=True, graph_launches=2)
     att = (b.n_accepted + b.n_rejected).cpu().numpy()
     assert att.max() <= 200
+
+
+def test_autotune_picks_a_guarded_config_and_keeps_results():
+    """The tuner times its candidates on the post-tip fixture, applies the
+    winner, and the tuned trace agrees with the default one (round size and
+    rule thresholds change rounding only: within the mixed form's 1e-6)."""
+    from conftest import load_golden
+    from bem_b200 import autotune
+
+    g = load_golden("trace_post")
+    spec = dict(kind="post_bem", E_gun=float(g["E_gun"]), R=float(g["R"]), L=float(g["L"]), z0=float(g["z0"]),
+                profile=g["profile"], sigma=g["sigma"], n_subdiv=int(g["n_subdiv"]), z_handoff=float(g["z_handoff"]),
+                kill_z_below=0.0)
+    geo = gu.device_geometry(spec)
+    G, E, _ = g["pos0"].shape
+    arrays = (g["pos0"].reshape(-1, 3), g["vel0"].reshape(-1, 3), g["t_birth"].reshape(-1),
+              np.full(G * E, gu.Q_E), np.full(G * E, gu.M_E), [E] * G)
+    args = (float(g["t_max"]), 1e-8, 1e-12, 1e-12, gu.CM)
+
+    def trace(tuned):
+        tr = engine.Tracer(geo, form="mixed", z_max=float(g["z_max"]), far_rule="adaptive")
+        b = engine.GroupBatch(*arrays)
+        res = None
+        if tuned:
+            res = autotune.tune(tr, *arrays, *args, warm=8, attempts=4)
+            autotune.apply(res, tr, b)
+        tr.launch(b, tr.params(*args, 30))
+        torch.cuda.synchronize()
+        return b.positions().cpu().numpy(), res
+
+    p_ref, _ = trace(False)
+    p, res = trace(True)
+    assert res["round_points"] in autotune.ROUND_POINTS and res["order"] in autotune.ORDERS
+    assert tuple(res["ratios"]) in autotune.RATIOS
+    assert any(isinstance(v, float) for v in res["timings"].values())
+    # mixed form: a different round size reorders float32 sums, so the two
+    # traces agree to the form's 1e-6 bar, not bit for bit
+    assert np.abs(p - p_ref).max() <= 1e-6 * np.abs(p_ref).max()
