@@ -40,6 +40,7 @@ namespace spt {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kRound = 8;           // points per far-sum round
+constexpr double kKappa = 16.0;     // default conditioning bound of the mixed form's float32 sums
 constexpr int kTileNodes = 2048;    // nodes per TMA tile row (largest; halved while shared memory is short)
 constexpr size_t kMaxSmem = 226 * 1024;  // dynamic part; the static __shared__ scalars take the rest of 227 KB
 constexpr int kSmallGroup = 256;    // groups above this keep slopes in global memory
@@ -191,7 +192,7 @@ struct Layout {
     int sur;                  // surrogate region: act (4096), wt (4096), sout 2E, sseg E, st E, sd E, feat 128; -1 if none
     int tiles;                // 2 * 3 * tile_cap
     int tile_cap;             // nodes per TMA tile row
-    int red;                  // kWarps * 2 * kRound
+    int red;                  // kWarps * 3 * kRound (far-round reduction: E_rho, E_z, sum of |terms|)
     int ints;                 // int region start (in doubles)
     int total_doubles;
     int live_off, list_off, flags_off;  // in ints from ints start
@@ -234,7 +235,7 @@ __host__ __device__ inline Layout make_layout(int E, bool want_tiles, bool want_
         o = base;
         L.tile_cap = cap;
         L.tiles = o; o += want_tiles ? 2 * 3 * cap : 0;
-        L.red = o; o += kWarps * 2 * kRound;
+        L.red = o; o += kWarps * 3 * kRound;
         L.ints = o;
         L.total_doubles = o + (n_ints + 1) / 2;
         L.bytes = (size_t)L.total_doubles * 8 + 64;  // + mbarriers
@@ -257,6 +258,8 @@ struct Ctx {
     double soft2;    // plummer^2
     int form;
     int round_pts;           // points per far-sum round, 1..kRound
+    double kappa;            // mixed form: float32 sums whose sum of |terms| exceeds kappa x |result| are redone in float64
+    int* redo;               // shared flag of that test
     int E;
     double* base;    // dynamic smem
     Layout L;
@@ -278,7 +281,7 @@ struct Ctx {
     unsigned long long* sstats;
     uint32_t tmem;
     uint32_t key;               // hash key of the current stage evaluation (spot checks)
-    unsigned long long cnt[8];  // per-thread counter partials (thread 0 flushes)
+    unsigned long long cnt[SPT_N_COUNTERS];  // per-thread counter partials (flushed by flush_counters)
 };
 
 __device__ inline void bind(Ctx& c, double* smem, int E, double* slot, bool sur = false) {
@@ -286,6 +289,7 @@ __device__ inline void bind(Ctx& c, double* smem, int E, double* slot, bool sur 
     c.E = E;
     c.L = make_layout(E, true, sur);
     c.round_pts = kRound;
+    c.kappa = kKappa;
     const Layout& L = c.L;
     if (!L.big) {
         c.y0 = smem + L.y0;
@@ -313,8 +317,9 @@ __device__ inline void bind(Ctx& c, double* smem, int E, double* slot, bool sur 
     c.live = ib + L.live_off;
     c.list = ib + L.list_off;
     c.nflag = reinterpret_cast<unsigned char*>(ib + L.flags_off);
+    c.redo = ib + L.flags_off + kRound * 256 / 4;  // first spare int after the near-flag bytes
     c.bars = reinterpret_cast<uint64_t*>(smem + L.total_doubles + 1);
-    for (int k = 0; k < 8; ++k) c.cnt[k] = 0;
+    for (int k = 0; k < SPT_N_COUNTERS; ++k) c.cnt[k] = 0;
     if (L.sur >= 0) {
         double* r = smem + L.sur;
         c.act = reinterpret_cast<uint8_t*>(r);
@@ -372,6 +377,52 @@ __device__ __forceinline__ double blk_lower(const SptBem& b, int q, double r, do
 __device__ __forceinline__ double blk_lmax(const SptBem& b, int q) { return __ldg(b.blk + 3 * b.blk_stride + q); }
 
 
+// Fixed-order block reduction of a far round's accumulators into record
+// slots 5, 6 (far + near sums).  Mixed form: the Kahan sums are folded in,
+// and when the sum of |float32 terms| at a point exceeds kappa times the
+// whole field there (uniform + perturbation), *c.redo is set -- the float32
+// result is then ill-conditioned (shielded regions, where the perturbation
+// cancels the uniform field) and the caller recomputes the round in float64.
+template <int NP, bool MIX>
+__device__ __forceinline__ void round_reduce(Ctx& c, int r0, int np_, double* ar, double* az, const float* fr,
+                                             const float* fz, const float* kr, const float* kz, const float* sa) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* P = c.bpt;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        if (MIX) {
+            ar[p] += (double)fr[p] - (double)kr[p];
+            az[p] += (double)fz[p] - (double)kz[p];
+        }
+        const double vr = warp_sum(ar[p]);
+        const double vz = warp_sum(az[p]);
+        const double va = MIX ? warp_sum((double)sa[p]) : 0.0;
+        if (lane == 0) {
+            c.red[warp * 3 * kRound + p] = vr;
+            c.red[warp * 3 * kRound + kRound + p] = vz;
+            c.red[warp * 3 * kRound + 2 * kRound + p] = va;
+        }
+    }
+    __syncthreads();
+    if (tid < np_) {
+        double sr = 0.0, sz = 0.0, sabs = 0.0;
+        for (int w = 0; w < kWarps; ++w) {
+            sr += c.red[w * 3 * kRound + tid];
+            sz += c.red[w * 3 * kRound + kRound + tid];
+            sabs += c.red[w * 3 * kRound + 2 * kRound + tid];
+        }
+        const int k = r0 + tid;
+        const double er = sr + P[8 * k + 7], ez = sz + c.fld[3 * k + 2];
+        P[8 * k + 5] = er;
+        P[8 * k + 6] = ez;
+        if (MIX) {
+            const double tz = ez + c.g.E_gun;
+            if (!(sabs <= c.kappa * sqrt(er * er + tz * tz))) atomicOr(c.redo, 1);
+        }
+    }
+    __syncthreads();
+}
+
 // One far-sum round for points r0..r0+np_-1 of the list (np_ <= NP): the
 // node table streams through shared memory in TMA tiles (double buffered);
 // each thread takes NQ nodes at a time, strided by the CTA width, against
@@ -380,7 +431,7 @@ template <int NP, int NQ, bool MIX>
 __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_tile, bool& ok,
                           unsigned long long& far_evals) {
     const SptBem& b = c.bem;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const int nseg = b.n_seg, nps = b.nodes_per_seg;
     const int tile_cap = c.L.tile_cap;
     double* P = c.bpt;
@@ -388,6 +439,7 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
     uint64_t* bars = c.bars;
     double pr[NP], pinv[NP], pz[NP], ar[NP], az[NP];
     float fr[NP], fz[NP], kr[NP], kz[NP], prf[NP], pinvf[NP];  // mixed form: Kahan sums and float copies
+    float sa[NP];                                               // mixed form: sum of |float32 terms|
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
         const int k = r0 + (p < np_ ? p : 0);
@@ -396,10 +448,11 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
         pz[p] = P[8 * k + 4];
         ar[p] = 0.0;
         az[p] = 0.0;
-        fr[p] = fz[p] = kr[p] = kz[p] = 0.0f;
+        fr[p] = fz[p] = kr[p] = kz[p] = sa[p] = 0.0f;
         prf[p] = (float)pr[p];
         pinvf[p] = (float)pinv[p];
     }
+    if (MIX && tid == 0) *c.redo = 0;  // ordered before the reduction's writes by the barriers between
     auto issue = [&](int t, int buf) {
         const int s_first = t * segs_per_tile;
         const int nn = min(segs_per_tile, nseg - s_first) * nps;
@@ -459,6 +512,7 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
                                     const float w = (float)wq[j];
                                     kahan_add(fr[p], kr[p], w * er);
                                     kahan_add(fz[p], kz[p], w * ez);
+                                    sa[p] += fabsf(w * er) + fabsf(w * ez);
                                 } else {
                                     double e64r, e64z;
                                     ring_field_far(pr[p], pinv[p], dz, rq[j], e64r, e64z);
@@ -491,31 +545,7 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
         if (tid == 0 && t + 2 < n_tiles) issue(t + 2, buf);
     }
     // fixed-order block reduction of the round's accumulators
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-        if (MIX) {
-            ar[p] += (double)fr[p] - (double)kr[p];
-            az[p] += (double)fz[p] - (double)kz[p];
-        }
-        const double vr = warp_sum(ar[p]);
-        const double vz = warp_sum(az[p]);
-        if (lane == 0) {
-            c.red[warp * 2 * kRound + p] = vr;
-            c.red[warp * 2 * kRound + kRound + p] = vz;
-        }
-    }
-    __syncthreads();
-    if (tid < np_) {
-        double sr = 0.0, sz = 0.0;
-        for (int w = 0; w < kWarps; ++w) {
-            sr += c.red[w * 2 * kRound + tid];
-            sz += c.red[w * 2 * kRound + kRound + tid];
-        }
-        const int k = r0 + tid;
-        P[8 * k + 5] = sr + P[8 * k + 7];
-        P[8 * k + 6] = sz + c.fld[3 * k + 2];
-    }
-    __syncthreads();
+    round_reduce<NP, MIX>(c, r0, np_, ar, az, fr, fz, kr, kz, sa);
 }
 
 // Adaptive far sum (SPT_FAR_ADAPTIVE) for points r0..r0+np_-1 of the list.
@@ -535,7 +565,7 @@ constexpr int kAdaptRuns = kAdaptSegs / SPT_BLOCK_SEGS;
 static_assert(kAdaptRuns == 32, "one warp classifies a chunk's runs");
 static_assert(3 * kAdaptSegs * sizeof(int) <= 2 * 3 * 256 * sizeof(double), "segment lists must fit the smallest tile region");
 static_assert(kAdaptSegs <= kRound * 256, "near masks must fit the near-flag bytes");
-static_assert(160 <= kWarps * 2 * kRound * 2, "run lists and counts fit the reduction scratch");
+static_assert(160 <= kWarps * 3 * kRound * 2, "run lists and counts fit the reduction scratch");
 
 template <int NP, int NQ, bool MIX>
 __device__ void far_adaptive(Ctx& c, int r0, int np_, unsigned long long& far_evals) {
@@ -555,6 +585,7 @@ __device__ void far_adaptive(Ctx& c, int r0, int np_, unsigned long long& far_ev
     int* Mcls = s_wc + 128;
     double pr[NP], pinv[NP], pz[NP], ar[NP], az[NP];
     float fr[NP], fz[NP], kr[NP], kz[NP], prf[NP], pinvf[NP];
+    float sa[NP];
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
         const int k = r0 + (p < np_ ? p : 0);
@@ -563,10 +594,11 @@ __device__ void far_adaptive(Ctx& c, int r0, int np_, unsigned long long& far_ev
         pz[p] = P[8 * k + 4];
         ar[p] = 0.0;
         az[p] = 0.0;
-        fr[p] = fz[p] = kr[p] = kz[p] = 0.0f;
+        fr[p] = fz[p] = kr[p] = kz[p] = sa[p] = 0.0f;
         prf[p] = (float)pr[p];
         pinvf[p] = (float)pinv[p];
     }
+    if (MIX && tid == 0) *c.redo = 0;  // ordered before the reduction's writes by the barriers between
     const double r4 = b.ratio4, r2 = b.ratio2;
     const double* cr = b.coarse;
     const double* cz = b.coarse + b.coarse_stride;
@@ -702,6 +734,7 @@ __device__ void far_adaptive(Ctx& c, int r0, int np_, unsigned long long& far_ev
                                 const float w = (float)wq[j];
                                 kahan_add(fr[p], kr[p], w * er);
                                 kahan_add(fz[p], kz[p], w * ez);
+                                sa[p] += fabsf(w * er) + fabsf(w * ez);
                             } else {
                                 double e64r, e64z;
                                 ring_field_far(pr[p], pinv[p], dz, rq[j], e64r, e64z);
@@ -721,31 +754,7 @@ __device__ void far_adaptive(Ctx& c, int r0, int np_, unsigned long long& far_ev
         }
         __syncthreads();  // the lists are rewritten by the next chunk
     }
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-        if (MIX) {
-            ar[p] += (double)fr[p] - (double)kr[p];
-            az[p] += (double)fz[p] - (double)kz[p];
-        }
-        const double vr = warp_sum(ar[p]);
-        const double vz = warp_sum(az[p]);
-        if (lane == 0) {
-            c.red[warp * 2 * kRound + p] = vr;
-            c.red[warp * 2 * kRound + kRound + p] = vz;
-        }
-    }
-    __syncthreads();
-    if (tid < np_) {
-        double sr = 0.0, sz = 0.0;
-        for (int w = 0; w < kWarps; ++w) {
-            sr += c.red[w * 2 * kRound + tid];
-            sz += c.red[w * 2 * kRound + kRound + tid];
-        }
-        const int k = r0 + tid;
-        P[8 * k + 5] = sr + P[8 * k + 7];
-        P[8 * k + 6] = sz + c.fld[3 * k + 2];
-    }
-    __syncthreads();
+    round_reduce<NP, MIX>(c, r0, np_, ar, az, fr, fz, kr, kz, sa);
 }
 
 // ---------------------------------------------------------------------------
@@ -913,23 +922,32 @@ __device__ void bem_sums(Ctx& c, int n, int* status_flag) {
     bool ok = true;
     for (int r0 = 0; r0 < n; r0 += c.round_pts) {
         const int np_ = min(c.round_pts, n - r0);
-        if (b.far_rule == SPT_FAR_ADAPTIVE) {
-            const bool mix = c.form != SPT_FORM_FP64;
-            if (np_ == 1) mix ? far_adaptive<1, 8, true>(c, r0, np_, far_evals) : far_adaptive<1, 8, false>(c, r0, np_, far_evals);
-            else if (np_ == 2) mix ? far_adaptive<2, 4, true>(c, r0, np_, far_evals) : far_adaptive<2, 4, false>(c, r0, np_, far_evals);
-            else if (np_ <= 4) mix ? far_adaptive<4, 2, true>(c, r0, np_, far_evals) : far_adaptive<4, 2, false>(c, r0, np_, far_evals);
-            else mix ? far_adaptive<8, 1, true>(c, r0, np_, far_evals) : far_adaptive<8, 1, false>(c, r0, np_, far_evals);
-            continue;
+        // mixed form (and the exact sums of the learned form): float32 first,
+        // float64 again for a round whose float32 sums are ill-conditioned
+        bool fp64 = c.form == SPT_FORM_FP64;
+        if (!fp64) {
+            if (b.far_rule == SPT_FAR_ADAPTIVE) {
+                if (np_ == 1) far_adaptive<1, 8, true>(c, r0, np_, far_evals);
+                else if (np_ == 2) far_adaptive<2, 4, true>(c, r0, np_, far_evals);
+                else if (np_ <= 4) far_adaptive<4, 2, true>(c, r0, np_, far_evals);
+                else far_adaptive<8, 1, true>(c, r0, np_, far_evals);
+            } else {
+                if (np_ == 1) far_round<1, 8, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                else if (np_ == 2) far_round<2, 4, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                else if (np_ <= 4) far_round<4, 2, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                else far_round<8, 1, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+            }
+            fp64 = *c.redo != 0;
+            // every thread has read the flag before the next round's float32 pass resets it
+            __syncthreads();
+            if (fp64 && tid == 0) ++c.cnt[SPT_CNT_FP64_ROUNDS];
         }
-        if (c.form != SPT_FORM_FP64) {  // mixed, and the exact sums of the learned form
-            if (np_ == 1)
-                far_round<1, 8, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            else if (np_ == 2)
-                far_round<2, 4, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            else if (np_ <= 4)
-                far_round<4, 2, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            else
-                far_round<8, 1, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+        if (!fp64) continue;
+        if (b.far_rule == SPT_FAR_ADAPTIVE) {
+            if (np_ == 1) far_adaptive<1, 8, false>(c, r0, np_, far_evals);
+            else if (np_ == 2) far_adaptive<2, 4, false>(c, r0, np_, far_evals);
+            else if (np_ <= 4) far_adaptive<4, 2, false>(c, r0, np_, far_evals);
+            else far_adaptive<8, 1, false>(c, r0, np_, far_evals);
         } else {
             if (np_ == 1)
                 far_round<1, 8, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
@@ -1216,7 +1234,8 @@ __device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
 // origin), then the rest in float32 with Kahan-compensated sums.
 template <bool MIX, typename SRC>
 __device__ __forceinline__ void pair_sum(const Ctx& c, int E, int j0, int jstep, double xi, double yi, double zi,
-                                         double qk, SRC src, double& fx, double& fy, double& fz) {
+                                         double qk, SRC src, double& fx, double& fy, double& fz,
+                                         double* sabs = nullptr) {
     // sources j0, j0 + jstep, ... (the callers split one target's sources over
     // the lanes of a warp and add the partial sums)
     if (!MIX) {
@@ -1235,7 +1254,7 @@ __device__ __forceinline__ void pair_sum(const Ctx& c, int E, int j0, int jstep,
         }
         fx = ax; fy = ay; fz = az;
     } else {
-        float ax = 0.f, ay = 0.f, az = 0.f, cx = 0.f, cy = 0.f, cz = 0.f;
+        float ax = 0.f, ay = 0.f, az = 0.f, cx = 0.f, cy = 0.f, cz = 0.f, sa = 0.f;
         const float soft2 = (float)c.soft2;
         for (int j = j0; j < E; j += jstep) {
             if (!c.live[j]) continue;
@@ -1248,7 +1267,9 @@ __device__ __forceinline__ void pair_sum(const Ctx& c, int E, int j0, int jstep,
             kahan_add(ax, cx, cf * dx);
             kahan_add(ay, cy, cf * dy);
             kahan_add(az, cz, cf * dz);
+            sa += fabsf(cf * dx) + fabsf(cf * dy) + fabsf(cf * dz);
         }
+        if (sabs) *sabs += sa;
         fx = (double)ax - (double)cx;
         fy = (double)ay - (double)cy;
         fz = (double)az - (double)cz;
@@ -1343,38 +1364,42 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
 
     // 3. per particle: field + pair sums.  Each target's sources are split
     // over T lanes of a warp (T = 256 / E rounded down to a power of two, at
-    // most 32), whose partial sums are added with shuffles.
+    // most 32), whose partial sums are added with shuffles.  Mixed form: the
+    // sums run in float32 first; a target whose sum of |float32 terms| / m
+    // exceeds kappa times its whole acceleration is summed again in float64.
     int T = 1;
     while (T < 32 && T * 2 * E <= kThreads) T *= 2;
     const int per_pass = kThreads / T;
     const int sub = tid & (T - 1);
-    unsigned long long pairs = 0;
+    const int lead = (tid & 31) & ~(T - 1);  // lane of the target's first sub-lane
+    unsigned long long pairs = 0, redone = 0;
     for (int base = 0; base < E; base += per_pass) {
         const int i = base + tid / T;
         const bool act = i < E && c.live[i];
-        double ax = 0.0, ay = 0.0, az = 0.0;
-        double fcx = 0.0, fcy = 0.0, fcz = 0.0, fix = 0.0, fiy = 0.0, fiz = 0.0;
         const bool mix = c.form != SPT_FORM_FP64;
         const int ii = i < E ? i : 0;
         const double xi = sx[ii], yi = sy[ii], zi = sz[ii];
         const double qk = c.kc * c.q[ii];
-        if (act) {
+        // this lane's share of the target's Coulomb (fc) and image (fi) sums
+        auto pass = [&](bool f32, bool on, double& fcx, double& fcy, double& fcz, double& fix, double& fiy,
+                        double& fiz, double& sabs) {
+            fcx = fcy = fcz = fix = fiy = fiz = sabs = 0.0;
+            if (!on) return;
+            double* sa = f32 ? &sabs : nullptr;
             if (E > 1) {
                 auto real = [&](int j, double& x, double& y, double& z, double& q) {
                     x = sx[j]; y = sy[j]; z = sz[j]; q = c.q[j];
                 };
-                if (mix) pair_sum<true>(c, E, sub, T, xi, yi, zi, qk, real, fcx, fcy, fcz);
+                if (f32) pair_sum<true>(c, E, sub, T, xi, yi, zi, qk, real, fcx, fcy, fcz, sa);
                 else pair_sum<false>(c, E, sub, T, xi, yi, zi, qk, real, fcx, fcy, fcz);
-                if (sub == 0) pairs += E;
             }
             if (KIND == SPT_GEOM_FLAT && g.has_image) {
                 const double zimg = -2.0 * g.z0;
                 auto mirror = [&](int j, double& x, double& y, double& z, double& q) {
                     x = sx[j]; y = sy[j]; z = zimg - sz[j]; q = -c.q[j];
                 };
-                if (mix) pair_sum<true>(c, E, sub, T, xi, yi, zi, qk, mirror, fix, fiy, fiz);
+                if (f32) pair_sum<true>(c, E, sub, T, xi, yi, zi, qk, mirror, fix, fiy, fiz, sa);
                 else pair_sum<false>(c, E, sub, T, xi, yi, zi, qk, mirror, fix, fiy, fiz);
-                if (sub == 0) pairs += E;
             } else if (three_img) {
                 const double zc = (KIND == SPT_GEOM_POST_BEM) ? g.L : 0.0;
                 const double pz0 = (KIND == SPT_GEOM_POST_BEM) ? g.L + g.z0 : g.z0;
@@ -1389,10 +1414,10 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
                 auto plane_sphere = [&](int j, double& x, double& y, double& z, double& q) {
                     x = c.img[j]; y = c.img[E + j]; z = -2.0 * pz0 - c.img[2 * E + j]; q = -c.img[3 * E + j];
                 };
-                if (mix) {
-                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, sphere, s1x, s1y, s1z);
-                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, plane, s2x, s2y, s2z);
-                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, plane_sphere, s3x, s3y, s3z);
+                if (f32) {
+                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, sphere, s1x, s1y, s1z, sa);
+                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, plane, s2x, s2y, s2z, sa);
+                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, plane_sphere, s3x, s3y, s3z, sa);
                 } else {
                     pair_sum<false>(c, E, sub, T, xi, yi, zl, qk, sphere, s1x, s1y, s1z);
                     pair_sum<false>(c, E, sub, T, xi, yi, zl, qk, plane, s2x, s2y, s2z);
@@ -1401,14 +1426,23 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
                 fix = (s1x + s2x) + s3x;
                 fiy = (s1y + s2y) + s3y;
                 fiz = (s1z + s2z) + s3z;
-                if (sub == 0) pairs += 3 * E;
             }
-        }
-        // every lane takes part in the shuffles (inactive ones add zeros)
-        fcx = group_sum(fcx, T); fcy = group_sum(fcy, T); fcz = group_sum(fcz, T);
-        fix = group_sum(fix, T); fiy = group_sum(fiy, T); fiz = group_sum(fiz, T);
+            // every lane takes part in the shuffles (lanes without work add zeros)
+        };
+        auto reduce = [&](double& fcx, double& fcy, double& fcz, double& fix, double& fiy, double& fiz,
+                          double& sabs) {
+            fcx = group_sum(fcx, T); fcy = group_sum(fcy, T); fcz = group_sum(fcz, T);
+            fix = group_sum(fix, T); fiy = group_sum(fiy, T); fiz = group_sum(fiz, T);
+            sabs = group_sum(sabs, T);
+        };
         if (act && sub == 0) {
-            double ex, ey, ez;
+            pairs += (E > 1 ? E : 0) + ((KIND == SPT_GEOM_FLAT && g.has_image) ? E : 0) + (three_img ? 3 * E : 0);
+        }
+        double fcx, fcy, fcz, fix, fiy, fiz, sabs;
+        pass(mix, act, fcx, fcy, fcz, fix, fiy, fiz, sabs);
+        reduce(fcx, fcy, fcz, fix, fiy, fiz, sabs);
+        double ex = 0.0, ey = 0.0, ez = 0.0;
+        if (act && sub == 0) {
             if (KIND == SPT_GEOM_FLAT) {
                 ex = 0.0; ey = 0.0; ez = (zi >= 0.0) ? g.E_gun : 0.0;
             } else if (KIND == SPT_GEOM_TIP) {
@@ -1430,10 +1464,27 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
                 ey = w * ny + (1.0 - w) * 0.0;
                 ez = w * nz + (1.0 - w) * fz;
             }
-            const double mi = c.m[i];
+        }
+        const double mi = act ? c.m[i] : 1.0;
+        auto accel_of = [&](double& ax, double& ay, double& az) {
             ax = (c.cm * ex + fcx / mi) + fix / mi;
             ay = (c.cm * ey + fcy / mi) + fiy / mi;
             az = (c.cm * ez + fcz / mi) + fiz / mi;
+        };
+        double ax = 0.0, ay = 0.0, az = 0.0;
+        bool redo = false;
+        if (act && sub == 0) {
+            accel_of(ax, ay, az);
+            redo = mix && !(sabs / mi <= c.kappa * sqrt(ax * ax + ay * ay + az * az));
+        }
+        redo = __shfl_sync(0xffffffffu, redo, lead);
+        if (__any_sync(0xffffffffu, redo)) {
+            pass(false, act && redo, fcx, fcy, fcz, fix, fiy, fiz, sabs);
+            reduce(fcx, fcy, fcz, fix, fiy, fiz, sabs);
+            if (act && redo && sub == 0) {
+                accel_of(ax, ay, az);
+                ++redone;
+            }
         }
         if (i < E && sub == 0) {
             out[i] = ax;
@@ -1441,6 +1492,7 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
             out[2 * E + i] = az;
         }
     }
+    c.cnt[SPT_CNT_FP64_TARGETS] += redone;
     c.cnt[SPT_CNT_PAIR_EVALS] += pairs;
     __syncthreads();
 }
@@ -1610,10 +1662,12 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
     c.kc = prm.coulomb_constant;
     c.soft2 = prm.plummer_radius * prm.plummer_radius;
     c.form = prm.form;
-    c.round_pts = (prm.round_points >= 1 && prm.round_points <= kRound) ? prm.round_points : kRound;
     const int Emax = st.max_group_size;
     const bool sur = prm.form == SPT_FORM_SURROGATE;
     bind(c, smem, Emax, big_slots ? big_slots + (size_t)blockIdx.x * big_slot_doubles(Emax) : nullptr, sur);
+    // launch-configuration parameters (bind sets the defaults)
+    c.round_pts = (prm.round_points >= 1 && prm.round_points <= kRound) ? prm.round_points : kRound;
+    if (prm.kappa_max > 0.0) c.kappa = prm.kappa_max;
     __shared__ uint32_t s_tmem;
     if (sur) bind_surrogate(c, prm, &s_tmem);
     init_barriers(c);
@@ -1665,7 +1719,9 @@ trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* 
             if (gs.status == SPT_GROUP_NEW) {
                 gs.t = c.cps[0];
                 gs.h = (prm.t_max - gs.t) * prm.initial_step_fraction;
-                gs.status = SPT_GROUP_RUNNING;
+                // a group born entirely at or after t_max has nothing to integrate: it is
+                // done as it stands (the reference would take a backward step to t_max)
+                gs.status = gs.t < prm.t_max ? SPT_GROUP_RUNNING : SPT_GROUP_DONE;
                 // an output time equal to the start time fires here (batched_rk45.py:191-209)
                 if (prm.n_outputs > 0) {
                     const int last = count_le(prm.output_times, prm.n_outputs, gs.t) - 1;
@@ -1899,6 +1955,7 @@ bem_field_kernel(const double* x, const double* y, const double* z, long long n,
     extern __shared__ __align__(16) double smem[];
     __shared__ int s_flag;
     Ctx c;
+    c.g = SptGeometry{};
     c.bem = bem;
     c.form = form;
     bind(c, smem, kFieldChunk, nullptr);

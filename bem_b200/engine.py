@@ -172,6 +172,7 @@ class Tracer:
         self.tables = geometry.bem_tables(self.device) if geometry.is_bem else None
         self.far_rule = far_rule
         self.round_points = 0  # far-sum points per round (0: the kernel's default, 8); see autotune
+        self.kappa_max = 0.0   # mixed form's conditioning bound for float32 sums (0: the kernel's default, 16)
         self.bem = None
         if self.tables is not None:
             kw = {k: v for k, v in (("ratio4", ratio4), ("ratio2", ratio2), ("ratio_run", ratio_run)) if v is not None}
@@ -186,9 +187,10 @@ class Tracer:
 
     def params(self, t_max, rtol, atol, plummer_radius, charge_to_mass, max_attempts, log=None,
                safety=0.9, min_factor=0.2, max_factor=10.0, initial_step_fraction=1e-6,
-               coulomb_constant=COULOMB_CONSTANT, records=None, round_points=None):
+               coulomb_constant=COULOMB_CONSTANT, records=None, round_points=None, kappa_max=None):
         p = _lib.SptTraceParams()
         p.round_points = int(self.round_points if round_points is None else round_points)
+        p.kappa_max = float(self.kappa_max if kappa_max is None else kappa_max)
         p.t_max, p.rtol, p.atol = float(t_max), float(rtol), float(atol)
         p.plummer_radius = float(plummer_radius)
         p.charge_to_mass = float(charge_to_mass)

@@ -299,6 +299,7 @@ def run_gpu(args, rank, world):
     pos, vel, tb, q, m, cm = particle_arrays(wl["data"])
     sizes = wl["data"]["group_sizes"]
     tracer = engine.Tracer(wl["geometry"], device=dev, form=args.form, z_max=wl["z_max"], far_rule=args.far_rule)
+    tracer.kappa_max = args.kappa
     batch = engine.GroupBatch(pos, vel, tb, q, m, sizes, device=dev)
     tuned = None
     if args.tune:
@@ -407,6 +408,7 @@ def accuracy_leg(args, wl, pos, vel, tb, q, m, cm, sizes, dev):
     out = {}
     for form, rule in (("fp64", "reference"), (args.form, args.far_rule)):
         tracer = engine.Tracer(wl["geometry"], device=dev, form=form, z_max=wl["z_max"], far_rule=rule)
+        tracer.kappa_max = args.kappa
         batch = engine.GroupBatch(pos[:k], vel[:k], tb[:k], q[:k], m[:k], sizes[:n], device=dev)
         tracer.run(batch, args.acc_time, wl["rtol"], wl["atol"], 1e-12, cm)
         torch.cuda.synchronize()
@@ -490,6 +492,8 @@ def main():
     ap.add_argument("--groups", type=int, default=None, help="first N emission groups only (profiling a smaller case)")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain form beside the chosen one")
     ap.add_argument("--tune", action="store_true", help="autotune the launch configuration first (untimed)")
+    ap.add_argument("--kappa", type=float, default=0.0,
+                    help="mixed form: conditioning bound above which float32 sums are redone in float64 (0: 16)")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the endpoint-error leg")
     ap.add_argument("--acc-groups", type=int, default=64)
     ap.add_argument("--acc-time", type=float, default=20e-12, help="end time of the endpoint-error traces [s]")
@@ -529,7 +533,7 @@ def main():
         ms_per_step=mean_ms, higher_is_better=True, scaling="weak", vs_baseline=None,
         dtype="f64" if fp64 else "f32+f64", data="synthetic (seeded samplers, workloads.py)",
         config=dict(r["config"], form=args.form, far_rule=args.far_rule, attempts_per_step=args.attempts,
-                    autotuned=r["tuned"],
+                    kappa_max=args.kappa or 16.0, autotuned=r["tuned"],
                     parallelism=f"groups x {world} GPUs",
                     l2="flushed between steps (256 MiB write); each step timed alone with CUDA events"),
         clocks=r["clocks"], gpu_launches=args.steps,

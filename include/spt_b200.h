@@ -73,7 +73,9 @@ extern "C" {
 #define SPT_CNT_RING_FAR 5           /* far-quadrature ring-kernel evaluations */
 #define SPT_CNT_RING_NEAR 6          /* near (sinh-quadrature) ring-kernel evaluations */
 #define SPT_CNT_NEAR_PAIRS 7         /* (point, segment) pairs handled by the near quadrature */
-#define SPT_N_COUNTERS 8
+#define SPT_CNT_FP64_ROUNDS 8        /* mixed form: far-sum rounds recomputed in float64 (ill-conditioned) */
+#define SPT_CNT_FP64_TARGETS 9       /* mixed form: pair-sum targets recomputed in float64 */
+#define SPT_N_COUNTERS 10
 
 /* Geometry parameters.  Fields a kind does not use are ignored. */
 typedef struct {
@@ -238,6 +240,13 @@ typedef struct {
      * adaptive rule, to its ~1e-14 classification effect). */
     int32_t round_points;
     int32_t reserved2;
+    /* Mixed form: a float32 far-sum round or pair sum whose sum of |terms|
+     * exceeds kappa_max times the whole field (uniform included) or the
+     * whole acceleration at a point is recomputed in float64 -- the float32
+     * result would carry eps_f x that ratio of relative error (shielded
+     * regions, where the perturbation cancels the uniform field; dense
+     * bunches).  0: the default, 16. */
+    double kappa_max;
 } SptTraceParams;
 
 /* Scratch bytes spt_trace needs for this state/geometry (work-queue

@@ -118,3 +118,22 @@ def test_autotune_picks_a_guarded_config_and_keeps_results():
     # mixed form: a different round size reorders float32 sums, so the two
     # traces agree to the form's 1e-6 bar, not bit for bit
     assert np.abs(p - p_ref).max() <= 1e-6 * np.abs(p_ref).max()
+
+
+def test_group_born_after_t_max_is_done_untouched():
+    """A group whose every member is born after t_max has nothing to
+    integrate: it finishes with no attempt and its particles unchanged,
+    while the other groups of the launch run normally."""
+    pos, vel, tb, sizes = _uneven(n_groups=4)
+    tb = tb.copy()
+    first = slice(0, int(sizes[0]))
+    tb[first] = 5e-12  # the first group: born after t_max below
+    geo = gu.device_geometry(dict(kind="flat", E_gun=-1e7, z0=3e-9, kill_z_below=0.0))
+    tr = engine.Tracer(geo, z_max=2e-5)
+    n = len(pos)
+    b = engine.GroupBatch(pos, vel, tb, np.full(n, gu.Q_E), np.full(n, gu.M_E), sizes)
+    tr.run(b, 3e-12, 1e-8, 1e-12, 1e-12, gu.CM)
+    assert np.all(b.status.cpu().numpy() == _lib.GROUP_DONE)
+    assert int(b.n_accepted[0].item() + b.n_rejected[0].item()) == 0
+    np.testing.assert_array_equal(b.positions().cpu().numpy()[first], pos[first])
+    assert int(b.n_accepted[1:].sum().item()) > 0

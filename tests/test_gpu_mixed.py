@@ -75,3 +75,39 @@ def test_trace_mixed_tip_no_kill_1e6():
     out = gu.device_trace(spec, pos0, vel0, tb, 1.2e-12, 1e-9, 1e-12, None, form="mixed")
     assert np.abs(out["pos"] - p).max() / np.abs(p).max() <= 1e-6
     assert np.abs(out["vel"] - v).max() / np.abs(v).max() <= 1e-6
+
+
+def _post_trace(form, far_rule="adaptive", attempts=40, **tracer_attrs):
+    g = load_golden("trace_post")
+    spec = dict(kind="post_bem", E_gun=float(g["E_gun"]), R=float(g["R"]), L=float(g["L"]), z0=float(g["z0"]),
+                profile=g["profile"], sigma=g["sigma"], n_subdiv=int(g["n_subdiv"]), z_handoff=float(g["z_handoff"]),
+                kill_z_below=0.0)
+    G, E, _ = g["pos0"].shape
+    tr = engine.Tracer(gu.device_geometry(spec), form=form, z_max=float(g["z_max"]), far_rule=far_rule)
+    for k, v in tracer_attrs.items():
+        setattr(tr, k, v)
+    b = engine.GroupBatch(g["pos0"].reshape(-1, 3), g["vel0"].reshape(-1, 3), g["t_birth"].reshape(-1),
+                          np.full(G * E, gu.Q_E), np.full(G * E, gu.M_E), [E] * G)
+    tr.launch(b, tr.params(float(g["t_max"]), 1e-8, 1e-12, 1e-12, gu.CM, attempts))
+    torch.cuda.synchronize()
+    return b.positions().cpu().numpy(), tr.counter_dict()
+
+
+@pytest.mark.parametrize("far_rule", ["reference", "adaptive"])
+def test_mixed_form_redoes_ill_conditioned_sums_in_float64(far_rule):
+    """kappa_max -> 0 declares every float32 sum ill-conditioned: every far
+    round and pair sum is recomputed by the float64 code, so the mixed form
+    reproduces the float64 form exactly."""
+    p64, _ = _post_trace("fp64", far_rule)
+    pmx, c = _post_trace("mixed", far_rule, kappa_max=1e-300)
+    assert c["fp64_rounds"] > 0 and c["fp64_targets"] > 0
+    np.testing.assert_array_equal(pmx, p64)
+
+
+def test_round_points_changes_the_far_tile_only():
+    """A far-sum round of 2 points instead of 8: other summation order and
+    classification rounds, same trace to 1e-10."""
+    p8, _ = _post_trace("fp64", "adaptive")
+    p2, _ = _post_trace("fp64", "adaptive", round_points=2)
+    assert not np.array_equal(p2, p8)
+    np.testing.assert_allclose(p2, p8, rtol=1e-10, atol=1e-10 * np.abs(p8).max())
