@@ -3,11 +3,13 @@ tracer's hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
                     [--workload c1|c0|c2|c3|c4] [--attempts A] [--form fp64|mixed]
-                    [--far-rule reference|adaptive]
+                    [--far-rule reference|adaptive] [--no-tune]
 
 The chosen form (the default): float32 + Kahan BEM and pair sums (float64
 state, stage combination, error norm and controller, float64 for points
-close to a ring) with the adaptive far-field rule.  The plain form (float64,
+close to a ring and for ill-conditioned sums) with the adaptive far-field
+rule, its launch configuration chosen first by the project's autotuner on a
+sample of the workload (untimed; `--no-tune` keeps the defaults).  The plain form (float64,
 the reference's quadrature) is timed in the same run on the same workload
 (`plain_fp64`), and `accuracy` reports the chosen form's endpoint error
 against it on a sample of groups traced to a fixed time.
@@ -309,6 +311,7 @@ def run_gpu(args, rank, world):
         res = autotune.tune(tracer, pos, vel, tb, q, m, sizes, wl["t_max"], wl["rtol"], wl["atol"], 1e-12, cm)
         autotune.apply(res, tracer, batch)
         tracer.tuned_order = res["order"]
+        args.tuned_config = res
         tuned = dict(res, seconds=round(time.perf_counter() - t0, 2), sample_groups=res.get("sample_groups"),
                      timings={k: (round(v) if isinstance(v, float) else v) for k, v in res.get("timings", {}).items()})
     stream = torch.cuda.current_stream(dev)
@@ -410,6 +413,9 @@ def accuracy_leg(args, wl, pos, vel, tb, q, m, cm, sizes, dev):
         tracer = engine.Tracer(wl["geometry"], device=dev, form=form, z_max=wl["z_max"], far_rule=rule)
         tracer.kappa_max = args.kappa
         batch = engine.GroupBatch(pos[:k], vel[:k], tb[:k], q[:k], m[:k], sizes[:n], device=dev)
+        if (form, rule) == (args.form, args.far_rule) and getattr(args, "tuned_config", None):
+            from bem_b200 import autotune
+            autotune.apply(args.tuned_config, tracer, batch)  # the chosen form as timed
         tracer.run(batch, args.acc_time, wl["rtol"], wl["atol"], 1e-12, cm)
         torch.cuda.synchronize()
         c = tracer.counter_dict()
@@ -491,7 +497,9 @@ def main():
     ap.add_argument("--cpu-attempts", type=int, default=16)
     ap.add_argument("--groups", type=int, default=None, help="first N emission groups only (profiling a smaller case)")
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain form beside the chosen one")
-    ap.add_argument("--tune", action="store_true", help="autotune the launch configuration first (untimed)")
+    ap.add_argument("--tune", dest="tune", action="store_true", default=True,
+                    help="autotune the launch configuration first (untimed; the default)")
+    ap.add_argument("--no-tune", dest="tune", action="store_false", help="time the default launch configuration")
     ap.add_argument("--kappa", type=float, default=0.0,
                     help="mixed form: conditioning bound above which float32 sums are redone in float64 (0: 16)")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the endpoint-error leg")
