@@ -288,6 +288,21 @@ def fp32_peak_tflops(torch, dev, n=8192):
         torch.backends.cuda.matmul.allow_tf32 = old
 
 
+def combine_ranks(t_total, particle_steps, world, device):
+    """Whole-job numbers of a weak-scaling run: the slowest rank's timed
+    region (max) and the particle-steps of all ranks (sum), by collectives
+    on the initialised process group (NCCL on the GPU path; any backend)."""
+    if world == 1:
+        return float(t_total), float(particle_steps)
+    import torch
+    import torch.distributed as dist
+    tt = torch.tensor([float(t_total)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    st = torch.tensor([float(particle_steps)], dtype=torch.float64, device=device)
+    dist.all_reduce(st)
+    return float(tt.item()), float(st.item())
+
+
 def run_gpu(args, rank, world):
     import torch
     from bem_b200 import engine
@@ -342,14 +357,7 @@ def run_gpu(args, rank, world):
     c1 = tracer.counter_dict()
     dc = {k: c1[k] - c0[k] for k in c1}
     t_total = float(np.sum(times))
-    if world > 1:
-        tt = torch.tensor([t_total], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        steps_t = torch.tensor([float(dc["particle_steps"])], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(steps_t)
-        t_max_ranks, steps_all = float(tt.item()), float(steps_t.item())
-    else:
-        t_max_ranks, steps_all = t_total, float(dc["particle_steps"])
+    t_max_ranks, steps_all = combine_ranks(t_total, dc["particle_steps"], world, dev)
 
     # end-to-end leg: host (pinned) state in, host state out, every step
     e2e = None
