@@ -133,9 +133,11 @@ def log_uniform_sizes(rng, n_groups, lo, hi):
     return np.clip(np.rint(np.exp(rng.uniform(np.log(lo), np.log(hi), n_groups))), lo, hi).astype(np.int64)
 
 
-def well_c3(n_groups=65536, seed=3, R=2e-6, H=1e-6, max_size=256, mte_ev=0.05, t_spread=10e-12):
+def well_c3(n_groups=65536, seed=3, R=2e-6, H=1e-6, max_size=256, mte_ev=0.05, t_spread=10e-12, sizes=None):
+    """``sizes``: fixed group sizes instead of the log-uniform draw (one
+    size bin at a time, for fixtures of a per-size reference run)."""
     rng = np.random.default_rng(seed)
-    sizes = log_uniform_sizes(rng, n_groups, 1, max_size)
+    sizes = log_uniform_sizes(rng, n_groups, 1, max_size) if sizes is None else np.asarray(sizes, dtype=np.int64)
     n = int(sizes.sum())
     r = R * np.sqrt(rng.uniform(0.0, 1.0, n))
     ph = rng.uniform(0.0, 2.0 * np.pi, n)
@@ -144,9 +146,11 @@ def well_c3(n_groups=65536, seed=3, R=2e-6, H=1e-6, max_size=256, mte_ev=0.05, t
     return _pack(r * np.cos(ph), r * np.sin(ph), np.full(n, -H), px, py, pz, t, sizes)
 
 
-def tip_c4(profile, sigma, n_groups=65536, seed=4, R=50e-9, L=5e-6, max_size=128, ke_max=0.5, t_spread=1e-12):
+def tip_c4(profile, sigma, n_groups=65536, seed=4, R=50e-9, L=5e-6, max_size=128, ke_max=0.5, t_spread=1e-12,
+           sizes=None):
+    """``sizes``: fixed group sizes instead of the log-uniform draw."""
     rng = np.random.default_rng(seed)
-    sizes = log_uniform_sizes(rng, n_groups, 1, max_size)
+    sizes = log_uniform_sizes(rng, n_groups, 1, max_size) if sizes is None else np.asarray(sizes, dtype=np.int64)
     n = int(sizes.sum())
     pos, normal = _cap_sites(rng, n, R, L, sigma_on_cap(profile, sigma, R, L))
     mom = _lambertian_momenta(rng, normal, ke_max)

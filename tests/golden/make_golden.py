@@ -4,7 +4,9 @@ Run in the development container, where the reference package
 (``specific_particle_tracer`` from AdamCBartnik/BEM) is importable from its
 source tree:
 
-    python tests/golden/make_golden.py [--ref /path/to/reference] [names...]
+    python tests/golden/make_golden.py --ref <reference source tree> [names...]
+
+(or SPT_REFERENCE=<tree> instead of --ref)
 
 It puts ``tests/golden/_stub`` (a minimal ParticleGroup stand-in, since
 openpmd-beamphysics is not installed) and the reference tree on sys.path,
@@ -144,11 +146,15 @@ class _PostTip:
     flat fallback (bem.geometry._blend_with_flat_fallback), 3-image force of
     forces.hemispherical_tip_image_force in the apex frame."""
 
-    def __init__(self, E_gun, R, L, profile, z0, z_handoff, n_subdiv=8):
+    def __init__(self, E_gun, R, L, profile, z0, z_handoff, n_subdiv=8, sigma=None):
         from specific_particle_tracer.bem.axisymmetric import AxisymmetricBEMSolution
         from specific_particle_tracer.fields import GunField
         self.E_gun, self.R, self.L, self.z0, self.z_handoff, self.n_subdiv = E_gun, R, L, z0, z_handoff, n_subdiv
-        self.solution = AxisymmetricBEMSolution.solve(profile, dirichlet_fn=lambda rho, z: E_gun * z)
+        if sigma is None:
+            self.solution = AxisymmetricBEMSolution.solve(profile, dirichlet_fn=lambda rho, z: E_gun * z)
+        else:
+            # a density the reference solved earlier (sigma_c1.npz: 221 s to solve)
+            self.solution = AxisymmetricBEMSolution(np.asarray(profile, dtype=float), np.asarray(sigma, dtype=float))
         self.gun = GunField(E_gun)
 
     def inside(self, pos):
@@ -327,20 +333,186 @@ def gen_sigma_c1():
     _save("sigma_c1", profile=prof, sigma=sol.sigma, E_gun=-1e6)
 
 
+# ---------------------------------------------------------------------------
+# Fixtures at the benchmark configurations (C1-C4 scale: 2000- and
+# ~3000-panel BEM solutions, groups of 32 and 1024 particles, uneven sizes).
+# Each group is traced by its own call of the reference's integrate, in a
+# pool of processes: groups never interact in the reference (one group per
+# call gives the numbers a batched call gives), and the per-point BEM sums
+# make a 2000-panel trace cost ~10 ms per particle-stage on one core.
+
+def _one_group(job):
+    """Reference integrate on one group, for at most max_attempts attempts
+    (None: to t_max).  The state after the last accepted step, the death
+    times, the accepted step end times and the attempt count are rebuilt
+    from on_step and the counted accel calls, exactly as integrate applies
+    them (kill after an accepted step, only for particles active at its
+    start; batched_rk45.py:260-293)."""
+    from specific_particle_tracer import batched_rk45, geometry as g
+    from specific_particle_tracer.constants import ELEMENTARY_CHARGE, ev_to_kg
+    pos0, vel0, tb, t_max, rtol, atol, z_max, max_attempts = job
+    geo = _POOL_GEO  # set before the pool forks (geometry objects hold modules, which do not pickle)
+    E = pos0.shape[1]
+    m = ev_to_kg(510998.95069)
+    acc = g.make_accel_fn(np.full((1, E), -ELEMENTARY_CHARGE), np.full((1, E), m), -ELEMENTARY_CHARGE / m, geo, 1e-12)
+    calls = [0]
+
+    def counted(pos, vel, active, gidx):
+        calls[0] += 1
+        return acc(pos, vel, active, gidx)
+
+    kill = g.make_kill_fn(geo, z_max)
+    st = dict(pos=pos0.copy(), vel=vel0.copy(), t=float(tb.min()), td=np.full((1, E), np.inf), t_acc=[])
+
+    def on_step(gi, t_old, p_old, v_old, t_new, p_new, v_new):
+        was = (t_old[:, None] >= tb) & (t_old[:, None] < st["td"])
+        newly = was & kill(p_new)
+        st["td"] = np.where(newly, t_new[:, None], st["td"])
+        st["pos"], st["vel"], st["t"] = p_new.copy(), v_new.copy(), float(t_new[0])
+        st["t_acc"].append(float(t_new[0]))
+
+    t0 = time.time()
+    done = True
+    try:
+        batched_rk45.integrate(counted, pos0, vel0, tb, t_max, rtol, atol, on_step=on_step, kill_fn=kill,
+                               max_steps=max_attempts if max_attempts else 10_000_000)
+    except RuntimeError:
+        done = False  # the attempt budget ran out: the state after max_attempts attempts
+    return dict(pos=st["pos"][0], vel=st["vel"][0], t=st["t"], t_death=st["td"][0], attempts=calls[0] // 7,
+                n_acc=len(st["t_acc"]), t_acc=np.asarray(st["t_acc"]), done=done, seconds=time.time() - t0)
+
+
+_POOL_GEO = None
+
+
+def _trace_groups(geo, pos0, vel0, tb, t_max, rtol, atol, z_max, max_attempts=None, procs=8):
+    import multiprocessing as mp
+    global _POOL_GEO
+    _POOL_GEO = geo
+    G = pos0.shape[0]
+    jobs = [(pos0[k:k + 1], vel0[k:k + 1], tb[k:k + 1], t_max, rtol, atol, z_max, max_attempts) for k in range(G)]
+    with mp.get_context("fork").Pool(min(procs, G)) as pool:
+        res = pool.map(_one_group, jobs)
+    n_acc = np.array([r["n_acc"] for r in res])
+    t_acc = np.zeros((G, max(1, n_acc.max())))
+    for k, r in enumerate(res):
+        t_acc[k, :len(r["t_acc"])] = r["t_acc"]
+    print(f"  {G} groups x {pos0.shape[1]}: attempts {[r['attempts'] for r in res]}, "
+          f"{max(r['seconds'] for r in res):.0f} s")
+    return dict(pos0=pos0, vel0=vel0, t_birth=tb, t_max=t_max, rtol=rtol, atol=atol, z_max=z_max,
+                max_attempts=-1 if max_attempts is None else max_attempts,
+                pos=np.stack([r["pos"] for r in res]), vel=np.stack([r["vel"] for r in res]),
+                t=np.array([r["t"] for r in res]), t_death=np.stack([r["t_death"] for r in res]),
+                attempts=np.array([r["attempts"] for r in res]), n_acc=n_acc, t_acc=t_acc,
+                done=np.array([r["done"] for r in res]))
+
+
+def _c1_geometry():
+    """The C1 tip (R = 50 nm on a 5 um post, 2000-panel capsule, E = -1e6
+    V/m, z0 = 3 nm, z_handoff = 20 (L + R)) with the density the reference
+    solved (sigma_c1.npz)."""
+    g = np.load(os.path.join(HERE, "sigma_c1.npz"))
+    R, L = 50e-9, 5e-6
+    return _PostTip(-1e6, R, L, g["profile"], 3e-9, 20 * (L + R), sigma=g["sigma"]), g
+
+
+def _vel(d, mass):
+    from specific_particle_tracer.constants import ev_c_to_si_momentum
+    return np.stack([ev_c_to_si_momentum(d[k]) / mass for k in ("px", "py", "pz")], -1)
+
+
+def _bench_groups(d, first, n, E):
+    from specific_particle_tracer.constants import ev_to_kg
+    sl = slice(first * E, (first + n) * E)
+    pos = np.stack([d["x"][sl], d["y"][sl], d["z"][sl]], -1).reshape(n, E, 3)
+    vel = _vel({k: d[k][sl] for k in ("px", "py", "pz")}, ev_to_kg(510998.95069)).reshape(n, E, 3)
+    return pos, vel, d["t"][sl].reshape(n, E)
+
+
+def _post_fields(geo, g):
+    return dict(profile=g["profile"], sigma=g["sigma"], R=geo.R, L=geo.L, E_gun=geo.E_gun, z0=geo.z0,
+                z_handoff=geo.z_handoff, n_subdiv=8)
+
+
+def gen_trace_c1():
+    """C1 exactly: the first 4 groups x 32 of the C1 sampler (seed 1, drawn
+    at the full 4096 x 32 size), traced from emission to t = 20 ps."""
+    from bem_b200 import workloads as w
+    geo, g = _c1_geometry()
+    d = w.tip_c1(g["profile"], g["sigma"], seed=1)
+    pos, vel, tb = _bench_groups(d, 0, 4, 32)
+    res = _trace_groups(geo, pos, vel, tb, 20e-12, 1e-9, 1e-12, 1e-3)
+    _save("trace_c1", **_post_fields(geo, g), **res)
+
+
+def gen_trace_c2():
+    """C2 scale: one group of 1024 from the C2 sampler (seed 2) on the C1
+    tip, every member born at t = 0 (so all 1024 interact from the first
+    stage), 6 attempts."""
+    from bem_b200 import workloads as w
+    geo, g = _c1_geometry()
+    d = w.tip_c2(n_groups=1, seed=2)
+    d["t"] = np.zeros_like(d["t"])
+    pos, vel, tb = _bench_groups(d, 0, 1, 1024)
+    res = _trace_groups(geo, pos, vel, tb, 20e-12, 1e-9, 1e-12, 1e-3, max_attempts=6)
+    _save("trace_c2", **_post_fields(geo, g), **res)
+
+
+def gen_trace_c4():
+    """C4 size bins on the C1 tip (C4 sampler, seed 4, fixed sizes): 8 groups
+    of 1, 4 of 2, 2 of 7 traced to t = 20 ps, one of 128 for 150 attempts.
+    One fixture per bin (the reference needs one size per call)."""
+    from bem_b200 import workloads as w
+    geo, g = _c1_geometry()
+    for E, n, att in ((1, 8, None), (2, 4, None), (7, 2, None), (128, 1, 150)):
+        d = w.tip_c4(g["profile"], g["sigma"], seed=4, sizes=[E] * n)
+        pos, vel, tb = _bench_groups(d, 0, n, E)
+        res = _trace_groups(geo, pos, vel, tb, 20e-12, 1e-9, 1e-12, 1e-3, max_attempts=att)
+        _save(f"trace_c4_s{E}", **_post_fields(geo, g), **res)
+
+
+def gen_trace_c3():
+    """C3 size bins on the reference's own ~3000-segment well (R = 2 um,
+    H = 1 um, E = -2.5e6 V/m, max_length H/980): the C3 sampler (seed 3,
+    fixed sizes), 8 groups of 1 and 4 of 2 traced to t = 30 ps, one group
+    each of 129 and 256 for 60 attempts."""
+    from specific_particle_tracer.bem.geometry import CylindricalWellBEMGeometry
+    from bem_b200 import workloads as w
+    R, H = 2e-6, 1e-6
+    t0 = time.time()
+    geo = CylindricalWellBEMGeometry(-2.5e6, R, H, field_max_length=H / 980)
+    sol = geo.field_solver.solution
+    print(f"  well solve ({len(sol.profile) - 1} segments): {time.time() - t0:.0f} s")
+    _save("sigma_c3", profile=sol.profile, sigma=sol.sigma, E_gun=-2.5e6, R=R, H=H, z_handoff=geo.z_handoff)
+    for E, n, att in ((1, 8, None), (2, 4, None), (129, 1, 60), (256, 1, 60)):
+        d = w.well_c3(seed=3, sizes=[E] * n)
+        pos, vel, tb = _bench_groups(d, 0, n, E)
+        res = _trace_groups(geo, pos, vel, tb, 30e-12, 1e-9, 1e-12, 2e-3, max_attempts=att)
+        _save(f"trace_c3_s{E}", profile=sol.profile, sigma=sol.sigma, R=R, H=H, E_gun=-2.5e6,
+              z_handoff=geo.z_handoff, n_subdiv=8, **res)
+
+
 GENERATORS = dict(sigma_c1=gen_sigma_c1, ellip=gen_ellip, ring=gen_ring, accel=gen_accel, bem_sphere=gen_bem_sphere,
                   bem_well=gen_bem_well, bem_post=gen_bem_post, trace_flat=gen_trace_flat,
                   trace_tip=gen_trace_tip, trace_tip_bem=gen_trace_bem, trace_post=gen_trace_post,
                   trace_well=gen_trace_well, tracker=gen_tracker,
-                  trace_flat_c0=lambda: gen_trace_flat(16))
+                  trace_flat_c0=lambda: gen_trace_flat(16), trace_c1=gen_trace_c1, trace_c2=gen_trace_c2,
+                  trace_c3=gen_trace_c3, trace_c4=gen_trace_c4)
+
+# generated only when named (minutes to an hour of CPU each)
+ON_REQUEST = ("trace_flat_c0", "sigma_c1", "trace_c1", "trace_c2", "trace_c3", "trace_c4")
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("SPT_REFERENCE"),
+                    help="source tree of the reference project (or set SPT_REFERENCE)")
     ap.add_argument("names", nargs="*")
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give the reference source tree with --ref or SPT_REFERENCE")
     _setup(a.ref)
-    for name in a.names or [k for k in GENERATORS if k not in ("trace_flat_c0", "sigma_c1")]:
+    for name in a.names or [k for k in GENERATORS if k not in ON_REQUEST]:
         t0 = time.time()
         GENERATORS[name]()
         print(f"{name}: {time.time() - t0:.1f}s")
