@@ -18,7 +18,7 @@ FAR_REFERENCE, FAR_ADAPTIVE = 0, 1
 FAR_RULES = {"reference": FAR_REFERENCE, "adaptive": FAR_ADAPTIVE}
 GROUP_NEW, GROUP_RUNNING, GROUP_DONE, GROUP_NONFINITE, GROUP_TIMEOUT = 0, 1, 2, 3, 4
 COUNTERS = ("attempts", "accepted", "particle_steps", "stage_evals", "pair_evals", "ring_far", "ring_near",
-            "near_pairs", "fp64_rounds", "fp64_targets")
+            "near_pairs", "fp64_rounds", "fp64_targets", "live_steps")
 N_COUNTERS = len(COUNTERS)
 SEG_FIELDS = 11
 BLOCK_SEGS = 32
@@ -61,7 +61,8 @@ class SptTraceParams(ctypes.Structure):
                 ("screen_capacity", _i64), ("screen_count", _p), ("output_times", _p), ("output_rec", _p),
                 ("output_flag", _p), ("sur_w", _p), ("sur_w16", _p), ("sur_s_start", _p), ("sur_log_scale", _p),
                 ("sur_s_end", _d), ("sur_sig_floor", _d), ("sur_band", _d), ("sur_spot", _d), ("sur_d_min", _d),
-                ("sur_d_max", _d), ("sur_stats", _p), ("round_points", _i32), ("reserved2", _i32), ("kappa_max", _d)]
+                ("sur_d_max", _d), ("sur_stats", _p), ("round_points", _i32), ("cta_threads", _i32), ("kappa_max", _d),
+                ("max_ctas", _i32), ("reserved3", _i32)]
 
 
 class SptAccelArgs(ctypes.Structure):

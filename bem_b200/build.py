@@ -13,14 +13,17 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libspt_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("spt_kernels.cu", "spt_mlp.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", h) for h in ("spt_math.cuh", "spt_umma.cuh")] + [
+SOURCES = [os.path.join(HERE, "csrc", f) for f in (
+    "spt_kernels.cu", "spt_mlp.cu", "spt_trace_flat.cu", "spt_trace_tip.cu", "spt_trace_tipbem.cu",
+    "spt_trace_well.cu", "spt_trace_post.cu")]
+DEPS = SOURCES + [os.path.join(HERE, "csrc", h) for h in ("spt_device.cuh", "spt_math.cuh", "spt_umma.cuh")] + [
     os.path.join(REPO, "include", "spt_b200.h")]
+OBJ_DIR = os.path.join(HERE, "_build")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-shared",
+    "-Xcompiler", "-fPIC",
     "-Xptxas", "-v",
 ]
 
@@ -40,14 +43,34 @@ def up_to_date():
 
 
 def build(force=False, verbose=False):
+    """Compile every translation unit (in parallel: one per geometry kind of
+    the trace kernel, the C ABI, the MLP kernels) and link the library."""
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + ["-I", os.path.join(REPO, "include"), "-o", LIB + ".tmp"] + SOURCES + ["-lcuda"]
+    from concurrent.futures import ThreadPoolExecutor
+    os.makedirs(OBJ_DIR, exist_ok=True)
+    inc = ["-I", os.path.join(REPO, "include")]
+
+    def compile_one(src):
+        obj = os.path.join(OBJ_DIR, os.path.basename(src) + ".o")
+        cmd = [nvcc()] + NVCC_FLAGS + inc + ["-c", "-o", obj, src]
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        return src, obj, cmd, res
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    for src, obj, cmd, res in results:
+        if verbose or res.returncode != 0:
+            sys.stderr.write(res.stdout + res.stderr)
+        if res.returncode != 0:
+            raise RuntimeError(f"nvcc failed ({res.returncode}): {' '.join(cmd)}")
+    cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp"] + [
+        r[1] for r in results]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if verbose or res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
     if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({res.returncode}): {' '.join(cmd)}")
+        raise RuntimeError(f"nvcc link failed ({res.returncode}): {' '.join(cmd)}")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

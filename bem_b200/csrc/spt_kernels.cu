@@ -1,6 +1,7 @@
-// B200 (sm_100a) kernels for the specific_particle_tracer hot path.
+// B200 (sm_100a) kernels for the specific_particle_tracer hot path: the C ABI.
 //
-// One persistent kernel (trace_kernel) advances emission groups through the
+// One persistent kernel (trace_kernel, spt_device.cuh; instantiated per
+// geometry kind in spt_trace_<kind>.cu) advances emission groups through the
 // per-group adaptive Dormand-Prince 5(4) integrator of batched_rk45.py.  A
 // CTA owns one group at a time (groups come from a device work queue); the
 // group's state, its seven stage slopes and the stage positions live in
@@ -11,1993 +12,80 @@
 //   * Plummer-softened Coulomb pair forces within the group (forces.py:16-57),
 //   * the image-charge pair forces (forces.py:60-191).
 //
-// BEM field of a list of points (bem_points):
-//   A. closest segment per point: one warp per point, lanes stride the
-//      segment table, warp-shuffle argmin (ties -> lowest index, the
-//      strict-< rule of bem/axisymmetric.py:127), on-surface offset;
-//   B. near segments (distance < segment length): found by a lane-parallel
-//      test + ballot; each near segment is integrated by the whole warp with
-//      the sinh-mapped Gauss-8 rule (lanes over interval x node);
-//   C. far sum: the Gauss-4 node table streams through shared memory in
-//      tiles copied by the TMA bulk engine (cp.async.bulk + mbarrier, double
-//      buffered); up to 8 points per round, every thread owns a strided
-//      slice of each tile and keeps 8 (E_rho, E_z) accumulators; near
-//      segments are skipped by a per-(point, segment) flag; one fixed-order
-//      block reduction per round (bit-reproducible run to run).
-#include <cuda_runtime.h>
-#include <stdint.h>
-#include <stdio.h>
-#include <string.h>
-#include <math.h>
+// This file holds the argument checks and launches of every entry point of
+// include/spt_b200.h, and the small kernels only they use (BEM field at
+// arbitrary points, compaction, ring field, elliptic integrals, BEM
+// collocation matrix).
+#include <mutex>
 #include <stdarg.h>
 
-#include "../../include/spt_b200.h"
-#include "spt_math.cuh"
-#include "spt_umma.cuh"
+#include "spt_device.cuh"
 
 namespace spt {
 
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
-constexpr int kRound = 8;           // points per far-sum round
-constexpr double kKappa = 16.0;     // default conditioning bound of the mixed form's float32 sums
-constexpr int kTileNodes = 2048;    // nodes per TMA tile row (largest; halved while shared memory is short)
-constexpr size_t kMaxSmem = 226 * 1024;  // dynamic part; the static __shared__ scalars take the rest of 227 KB
-constexpr int kSmallGroup = 256;    // groups above this keep slopes in global memory
-
-// Dormand-Prince 5(4) tableau (batched_rk45.py:30-50).
-__device__ __constant__ double kA[6][5] = {
-    {0, 0, 0, 0, 0},
-    {1.0 / 5, 0, 0, 0, 0},
-    {3.0 / 40, 9.0 / 40, 0, 0, 0},
-    {44.0 / 45, -56.0 / 15, 32.0 / 9, 0, 0},
-    {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729, 0},
-    {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656}};
-__device__ __constant__ double kB[6] = {35.0 / 384, 0.0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84};
-__device__ __constant__ double kE[7] = {71.0 / 57600, 0.0, -71.0 / 16695, 71.0 / 1920, -17253.0 / 339200, 22.0 / 525, -1.0 / 40};
-
-constexpr double kSpeedOfLight = 299792458.0;
-constexpr double kTiny = 2.2250738585072014e-308;  // np.finfo(float).tiny
-
-// ---------------------------------------------------------------------------
-// small helpers
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void tma_load_1d(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// Bounded wait on an mbarrier phase.  Returns false when the iteration limit
-// ran out (the caller flags the group instead of spinning forever).
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
-    uint32_t done = 0;
-    for (int it = 0; it < (1 << 22); ++it) {
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(done)
-            : "r"(smem_u32(bar)), "r"(phase)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-template <typename T>
-__device__ __forceinline__ T warp_sum(T v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// ---------------------------------------------------------------------------
-// geometry helpers (fields.py, geometry.py, bem/fields.py, bem/geometry.py)
-
-__device__ __forceinline__ bool well_contains(double rho, double z, const SptGeometry& g) {
-    const double R = g.R, H = g.H;
-    const double eps = 1e-6 * R;
-    bool solid = (rho >= R * (1.0 - 1e-6)) ? (z <= 0.0) : (z <= -H * (1.0 + 1e-6));
-    if (g.rim_fillet > 0.0) {
-        const double rf = g.rim_fillet, cr = R + rf, cz = -rf;
-        if (rho >= R - eps && rho <= R + rf + eps && z >= -rf - eps && z <= eps) solid = hypot(rho - cr, z - cz) <= rf;
-    }
-    if (g.bottom_fillet > 0.0) {
-        const double bf = g.bottom_fillet, cr = R - bf, cz = -H + bf;
-        if (rho <= R + eps && rho >= R - bf - eps && z <= -H + bf + eps && z >= -H - eps)
-            solid = hypot(rho - cr, z - cz) >= bf;
-    }
-    return solid;
-}
-
-__device__ __forceinline__ bool post_inside(double x, double y, double z, const SptGeometry& g) {
-    const double rk = g.R * (1.0 - 1e-6);
-    const double r2 = x * x + y * y;
-    const double zc = z - g.L;
-    return (r2 <= rk * rk && z <= g.L) || (r2 + zc * zc <= rk * rk);
-}
-
-template <int KIND>
-__device__ __forceinline__ bool kill_test(double x, double y, double z, const SptGeometry& g) {
-    bool k = false;
-    if (KIND == SPT_GEOM_FLAT) {
-        k = g.has_kill_below && z <= g.kill_z_below;
-    } else if (KIND == SPT_GEOM_TIP || KIND == SPT_GEOM_TIP_BEM) {
-        const double rk = g.R * (1.0 - 1e-6);
-        k = (x * x + y * y + z * z) <= rk * rk;
-        if (g.has_kill_below) k = k || (z <= g.kill_z_below);
-    } else if (KIND == SPT_GEOM_WELL_BEM) {
-        k = well_contains(sqrt(x * x + y * y), z, g);
-    } else {
-        k = post_inside(x, y, z, g);
-        if (g.has_kill_below) k = k || (z <= g.kill_z_below);
-    }
-    if (g.has_z_max) k = k || (z >= g.z_max);
-    return k;
-}
-
-// analytic tip field (fields.py:119-160)
-__device__ __forceinline__ void tip_field(double x, double y, double z, double Ez, double R, double& ex, double& ey,
-                                          double& ez) {
-    const double r = sqrt(x * x + y * y + z * z);
-    const bool ok = (r >= R * (1.0 - 1e-6)) && (z >= 0.0);
-    if (!ok) {
-        ex = ey = ez = 0.0;
-        return;
-    }
-    const double r3 = r * r * r;
-    const double r5 = r3 * r * r;
-    const double R3 = R * R * R;
-    ex = 3.0 * Ez * R3 * x * z / r5;
-    ey = 3.0 * Ez * R3 * y * z / r5;
-    ez = Ez * (1.0 - R3 / r3 + 3.0 * R3 * z * z / r5);
-}
-
-// BEM geometries: is the point in the field's valid (vacuum) region
-template <int KIND>
-__device__ __forceinline__ bool bem_valid(double x, double y, double z, const SptGeometry& g) {
-    if (KIND == SPT_GEOM_TIP_BEM) return (sqrt(x * x + y * y + z * z) >= g.R * (1.0 - 1e-6)) && (z >= 0.0);
-    if (KIND == SPT_GEOM_WELL_BEM) return !well_contains(sqrt(x * x + y * y), z, g);
-    return !post_inside(x, y, z, g) && (z >= 0.0);
-}
-
-__device__ __forceinline__ double blend_weight(double z, double zh) {
-    const double zlo = 0.5 * zh;
-    double s = (zh - z) / (zh - zlo);
-    s = fmin(fmax(s, 0.0), 1.0);
-    return s * s * (3.0 - 2.0 * s);
-}
-
-// ---------------------------------------------------------------------------
-// shared-memory layout of one CTA
-
-struct Layout {
-    // offsets in doubles from the start of dynamic shared memory
-    int y0, nw, sp, kp, kv;   // y0: 6E, nw: 6E, sp: 3E, kp/kv: 21E each
-    int tb, td, q, m, cps;    // E each
-    int fld;                  // 3E field
-    int img;                  // 4E sphere images
-    int bpt;                  // 8E per BEM list entry: x y z rho_e z_e near_r near_z (+1 pad)
-    int sur;                  // surrogate region: act (4096), wt (4096), sout 2E, sseg E, st E, sd E, feat 128; -1 if none
-    int tiles;                // 2 * 3 * tile_cap
-    int tile_cap;             // nodes per TMA tile row
-    int red;                  // kWarps * 3 * kRound (far-round reduction: E_rho, E_z, sum of |terms|)
-    int ints;                 // int region start (in doubles)
-    int total_doubles;
-    int live_off, list_off, flags_off;  // in ints from ints start
-    size_t bytes;
-    bool big;                 // slopes/y0/nw in global memory
-};
-
-__host__ __device__ inline Layout make_layout(int E, bool want_tiles, bool want_sur = false) {
-    Layout L;
-    const bool big = E > kSmallGroup;
-    int o = 0;
-    L.big = big;
-    if (!big) {
-        L.y0 = o; o += 6 * E;
-        L.nw = o; o += 6 * E;
-        L.kp = o; o += 21 * E;
-        L.kv = o; o += 21 * E;
-    } else {
-        L.y0 = L.nw = L.kp = L.kv = -1;
-    }
-    L.sp = o; o += 3 * E;
-    L.tb = o; o += E;
-    L.td = o; o += E;
-    L.q = o; o += E;
-    L.m = o; o += E;
-    L.cps = o; o += E;
-    L.fld = o; o += 3 * E;
-    L.img = o; o += 4 * E;
-    L.bpt = o; o += 8 * E;
-    if (want_sur) {
-        o = (o + 127) & ~127;  // 1 KiB alignment for the tensor-core operand tiles
-        L.sur = o; o += 8192 + 5 * E + 128;
-    } else {
-        L.sur = -1;
-    }
-    o = (o + 1) & ~1;  // 16-byte alignment for the TMA tiles
-    const int base = o;
-    const int n_ints = 2 * E + kRound * 256 / 4 + 4;  // live, list, near flags (bytes) packed in ints
-    for (int cap = kTileNodes; cap >= 256; cap >>= 1) {
-        o = base;
-        L.tile_cap = cap;
-        L.tiles = o; o += want_tiles ? 2 * 3 * cap : 0;
-        L.red = o; o += kWarps * 3 * kRound;
-        L.ints = o;
-        L.total_doubles = o + (n_ints + 1) / 2;
-        L.bytes = (size_t)L.total_doubles * 8 + 64;  // + mbarriers
-        if (L.bytes <= kMaxSmem) break;
-    }
-    L.live_off = 0;
-    L.list_off = E;
-    L.flags_off = 2 * E;
-    return L;
-}
-
-// global per-CTA slot for big groups: y0 6E, nw 6E, kp 21E, kv 21E
-__host__ __device__ inline size_t big_slot_doubles(int E) { return (size_t)54 * E; }
-
-struct Ctx {
-    SptGeometry g;
-    SptBem bem;
-    double cm;       // charge_to_mass
-    double kc;       // Coulomb constant 1/(4 pi eps0)
-    double soft2;    // plummer^2
-    int form;
-    int round_pts;           // points per far-sum round, 1..kRound
-    double kappa;            // mixed form: float32 sums whose sum of |terms| exceeds kappa x |result| are redone in float64
-    int* redo;               // shared flag of that test
-    int E;
-    double* base;    // dynamic smem
-    Layout L;
-    double *y0, *nw, *sp, *kp, *kv, *tb, *td, *q, *m, *cps, *fld, *img, *bpt, *tiles, *red;
-    int* live;
-    int* list;
-    unsigned char* nflag;
-    uint64_t* bars;
-    uint32_t phase[3];          // parity of the next phase to wait for on bars[0..2] (identical in every thread)
-    // learned form
-    uint8_t *act, *wt;          // BF16 operand tiles (activations, weights), canonical K-major, 32 KiB each
-    double *sout, *st, *sd;     // surrogate E (rho, z) per record; closest-point parameter and distance
-    int* sseg;                  // closest segment per record
-    float* feat;                // features of the current 128-row chunk
-    const float* sw;            // FP32 (BF16-rounded) parameters
-    const __nv_bfloat16* sw16;  // BF16 parameters
-    const double *s_start, *log_scale;
-    double s_end, sig_floor, band, spot, dmin, dmax;
-    unsigned long long* sstats;
-    uint32_t tmem;
-    uint32_t key;               // hash key of the current stage evaluation (spot checks)
-    unsigned long long cnt[SPT_N_COUNTERS];  // per-thread counter partials (flushed by flush_counters)
-};
-
-__device__ inline void bind(Ctx& c, double* smem, int E, double* slot, bool sur = false) {
-    c.base = smem;
-    c.E = E;
-    c.L = make_layout(E, true, sur);
-    c.round_pts = kRound;
-    c.kappa = kKappa;
-    const Layout& L = c.L;
-    if (!L.big) {
-        c.y0 = smem + L.y0;
-        c.nw = smem + L.nw;
-        c.kp = smem + L.kp;
-        c.kv = smem + L.kv;
-    } else {
-        c.y0 = slot;
-        c.nw = slot + 6 * E;
-        c.kp = slot + 12 * E;
-        c.kv = slot + 33 * E;
-    }
-    c.sp = smem + L.sp;
-    c.tb = smem + L.tb;
-    c.td = smem + L.td;
-    c.q = smem + L.q;
-    c.m = smem + L.m;
-    c.cps = smem + L.cps;
-    c.fld = smem + L.fld;
-    c.img = smem + L.img;
-    c.bpt = smem + L.bpt;
-    c.tiles = smem + L.tiles;
-    c.red = smem + L.red;
-    int* ib = reinterpret_cast<int*>(smem + L.ints);
-    c.live = ib + L.live_off;
-    c.list = ib + L.list_off;
-    c.nflag = reinterpret_cast<unsigned char*>(ib + L.flags_off);
-    c.redo = ib + L.flags_off + kRound * 256 / 4;  // first spare int after the near-flag bytes
-    c.bars = reinterpret_cast<uint64_t*>(smem + L.total_doubles + 1);
-    for (int k = 0; k < SPT_N_COUNTERS; ++k) c.cnt[k] = 0;
-    if (L.sur >= 0) {
-        double* r = smem + L.sur;
-        c.act = reinterpret_cast<uint8_t*>(r);
-        c.wt = reinterpret_cast<uint8_t*>(r + 4096);
-        c.sout = r + 8192;
-        c.st = c.sout + 2 * E;
-        c.sd = c.st + E;
-        c.sseg = reinterpret_cast<int*>(c.sd + E);
-        c.feat = reinterpret_cast<float*>(c.sd + 2 * E);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// BEM: segment table access
-
-struct Seg {
-    double p0r, p0z, tr, tz, len, ur, uz, nr, nz, s0, s1;
-};
-
-__device__ __forceinline__ double segf(const SptBem& b, int f, int s) { return __ldg(b.seg + (size_t)f * b.seg_stride + s); }
-
-// closest-point distance^2 of (rq, zq) to segment s (bem/axisymmetric.py:117-133,
-// 374-381), with no FMA contraction: the on-surface offset below is a
-// threshold test on this value, so it is rounded like the reference's.
-__device__ __forceinline__ double seg_dist2(const SptBem& b, int s, double rq, double zq) {
-    const double p0x = segf(b, 0, s), p0y = segf(b, 1, s), ax = segf(b, 2, s), ay = segf(b, 3, s);
-    const double ab = __dadd_rn(__dmul_rn(ax, ax), __dmul_rn(ay, ay));
-    double t = __ddiv_rn(__dadd_rn(__dmul_rn(__dadd_rn(rq, -p0x), ax), __dmul_rn(__dadd_rn(zq, -p0y), ay)), ab);
-    t = fmin(fmax(t, 0.0), 1.0);
-    const double cr = __dadd_rn(p0x, __dmul_rn(t, ax)), cz = __dadd_rn(p0y, __dmul_rn(t, ay));
-    const double dr = __dadd_rn(rq, -cr), dz = __dadd_rn(zq, -cz);
-    return __dadd_rn(__dmul_rn(dr, dr), __dmul_rn(dz, dz));
-}
-
-// near test of bem/axisymmetric.py:566-570 -> (near, projection, distance)
-__device__ __forceinline__ bool seg_near(const SptBem& b, int s, double re, double ze, double& proj, double& dist) {
-    const double p0r = segf(b, 0, s), p0z = segf(b, 1, s), L = segf(b, 4, s), ur = segf(b, 5, s), uz = segf(b, 6, s);
-    const double dr = re - p0r, dz = ze - p0z;
-    const double along = dr * ur + dz * uz;
-    proj = fmin(fmax(along, 0.0), L);
-    const double ar = dr - proj * ur, az = dz - proj * uz;
-    dist = sqrt(ar * ar + az * az);
-    return dist < L;
-}
-
-// Runs of SPT_BLOCK_SEGS consecutive segments (SptBem.blk): a lower bound of
-// the distance from (r, z) to every segment of run q, less a relative margin
-// that covers the rounding of this bound and of the table, and the run's
-// largest segment length.
-__device__ __forceinline__ double blk_lower(const SptBem& b, int q, double r, double z) {
-    const double cr = __ldg(b.blk + q), cz = __ldg(b.blk + b.blk_stride + q), rad = __ldg(b.blk + 2 * b.blk_stride + q);
-    const double dc = sqrt((r - cr) * (r - cr) + (z - cz) * (z - cz));
-    return dc - rad - 1e-9 * (dc + rad);
-}
-__device__ __forceinline__ double blk_lmax(const SptBem& b, int q) { return __ldg(b.blk + 3 * b.blk_stride + q); }
-
-
-// Fixed-order block reduction of a far round's accumulators into record
-// slots 5, 6 (far + near sums).  Mixed form: the Kahan sums are folded in,
-// and when the sum of |float32 terms| at a point exceeds kappa times the
-// whole field there (uniform + perturbation), *c.redo is set -- the float32
-// result is then ill-conditioned (shielded regions, where the perturbation
-// cancels the uniform field) and the caller recomputes the round in float64.
-template <int NP, bool MIX>
-__device__ __forceinline__ void round_reduce(Ctx& c, int r0, int np_, double* ar, double* az, const float* fr,
-                                             const float* fz, const float* kr, const float* kz, const float* sa) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double* P = c.bpt;
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-        if (MIX) {
-            ar[p] += (double)fr[p] - (double)kr[p];
-            az[p] += (double)fz[p] - (double)kz[p];
-        }
-        const double vr = warp_sum(ar[p]);
-        const double vz = warp_sum(az[p]);
-        const double va = MIX ? warp_sum((double)sa[p]) : 0.0;
-        if (lane == 0) {
-            c.red[warp * 3 * kRound + p] = vr;
-            c.red[warp * 3 * kRound + kRound + p] = vz;
-            c.red[warp * 3 * kRound + 2 * kRound + p] = va;
-        }
-    }
-    __syncthreads();
-    if (tid < np_) {
-        double sr = 0.0, sz = 0.0, sabs = 0.0;
-        for (int w = 0; w < kWarps; ++w) {
-            sr += c.red[w * 3 * kRound + tid];
-            sz += c.red[w * 3 * kRound + kRound + tid];
-            sabs += c.red[w * 3 * kRound + 2 * kRound + tid];
-        }
-        const int k = r0 + tid;
-        const double er = sr + P[8 * k + 7], ez = sz + c.fld[3 * k + 2];
-        P[8 * k + 5] = er;
-        P[8 * k + 6] = ez;
-        if (MIX) {
-            const double tz = ez + c.g.E_gun;
-            if (!(sabs <= c.kappa * sqrt(er * er + tz * tz))) atomicOr(c.redo, 1);
-        }
-    }
-    __syncthreads();
-}
-
-// One far-sum round for points r0..r0+np_-1 of the list (np_ <= NP): the
-// node table streams through shared memory in TMA tiles (double buffered);
-// each thread takes NQ nodes at a time, strided by the CTA width, against
-// all NP points (NP * NQ independent ring evaluations per iteration).
-template <int NP, int NQ, bool MIX>
-__device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_tile, bool& ok,
-                          unsigned long long& far_evals) {
-    const SptBem& b = c.bem;
-    const int tid = threadIdx.x;
-    const int nseg = b.n_seg, nps = b.nodes_per_seg;
-    const int tile_cap = c.L.tile_cap;
-    double* P = c.bpt;
-    double* tile[2] = {c.tiles, c.tiles + 3 * tile_cap};
-    uint64_t* bars = c.bars;
-    double pr[NP], pinv[NP], pz[NP], ar[NP], az[NP];
-    float fr[NP], fz[NP], kr[NP], kz[NP], prf[NP], pinvf[NP];  // mixed form: Kahan sums and float copies
-    float sa[NP];                                               // mixed form: sum of |float32 terms|
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-        const int k = r0 + (p < np_ ? p : 0);
-        pr[p] = P[8 * k + 3];
-        pinv[p] = pr[p] > 0.0 ? 1.0 / pr[p] : 0.0;
-        pz[p] = P[8 * k + 4];
-        ar[p] = 0.0;
-        az[p] = 0.0;
-        fr[p] = fz[p] = kr[p] = kz[p] = sa[p] = 0.0f;
-        prf[p] = (float)pr[p];
-        pinvf[p] = (float)pinv[p];
-    }
-    if (MIX && tid == 0) *c.redo = 0;  // ordered before the reduction's writes by the barriers between
-    auto issue = [&](int t, int buf) {
-        const int s_first = t * segs_per_tile;
-        const int nn = min(segs_per_tile, nseg - s_first) * nps;
-        const uint32_t bytes = (uint32_t)nn * 8u;
-        mbar_expect_tx(&bars[buf], 3u * bytes);
-        for (int row = 0; row < 3; ++row)
-            tma_load_1d(tile[buf] + row * tile_cap, b.node + (size_t)row * b.node_stride + (size_t)s_first * nps, bytes,
-                        &bars[buf]);
-    };
-    if (tid == 0) {
-        issue(0, 0);
-        if (n_tiles > 1) issue(1, 1);
-    }
-    for (int t = 0; t < n_tiles; ++t) {
-        const int buf = t & 1;
-        const int s_first = t * segs_per_tile;
-        const int ns = min(segs_per_tile, nseg - s_first);
-        for (int idx = tid; idx < np_ * ns; idx += kThreads) {
-            const int p = idx / ns, sl = idx - p * ns;
-            double proj, dist;
-            c.nflag[p * 256 + sl] = seg_near(b, s_first + sl, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4], proj, dist);
-        }
-        if (!mbar_wait(&bars[buf], c.phase[buf])) ok = false;
-        c.phase[buf] ^= 1u;
-        __syncthreads();
-        if (ok) {
-            const double* tr = tile[buf];
-            const double* tz = tr + tile_cap;
-            const double* tw = tz + tile_cap;
-            const int nn = ns * nps;
-            for (int q0 = tid; q0 < nn; q0 += kThreads * NQ) {
-                double rq[NQ], zq[NQ], wq[NQ];
-                int sl[NQ];
-                bool in[NQ];
-#pragma unroll
-                for (int j = 0; j < NQ; ++j) {
-                    const int q = q0 + j * kThreads;
-                    in[j] = q < nn;
-                    const int qq = in[j] ? q : 0;
-                    rq[j] = tr[qq];
-                    zq[j] = tz[qq];
-                    wq[j] = tw[qq];
-                    sl[j] = qq / nps;
-                }
-                if (MIX) {
-                    // float32 Kahan sums; pairs the float path declines (p < 1e-3 or
-                    // near the axis) are evaluated in float64
-#pragma unroll
-                    for (int p = 0; p < NP; ++p) {
-#pragma unroll
-                        for (int j = 0; j < NQ; ++j) {
-                            if (p < np_ && in[j] && !c.nflag[p * 256 + sl[j]]) {
-                                const double dz = pz[p] - zq[j];
-                                float er, ez;
-                                if (ring_far_f(prf[p], pinvf[p], (float)(pr[p] - rq[j]), (float)(pr[p] + rq[j]),
-                                               (float)dz, (float)rq[j], er, ez)) {
-                                    const float w = (float)wq[j];
-                                    kahan_add(fr[p], kr[p], w * er);
-                                    kahan_add(fz[p], kz[p], w * ez);
-                                    sa[p] += fabsf(w * er) + fabsf(w * ez);
-                                } else {
-                                    double e64r, e64z;
-                                    ring_field_far(pr[p], pinv[p], dz, rq[j], e64r, e64z);
-                                    ar[p] = fma(wq[j], e64r, ar[p]);
-                                    az[p] = fma(wq[j], e64z, az[p]);
-                                }
-                                ++far_evals;
-                            }
-                        }
-                    }
-                } else {
-#pragma unroll
-                for (int p = 0; p < NP; ++p) {
-#pragma unroll
-                    for (int j = 0; j < NQ; ++j) {
-                        if (p < np_ && in[j] && !c.nflag[p * 256 + sl[j]]) {
-                            const double dz = pz[p] - zq[j];
-                            double er, ez;
-                            ring_field_far(pr[p], pinv[p], dz, rq[j], er, ez);
-                            ar[p] = fma(wq[j], er, ar[p]);
-                            az[p] = fma(wq[j], ez, az[p]);
-                            ++far_evals;
-                        }
-                    }
-                }
-                }
-            }
-        }
-        __syncthreads();
-        if (tid == 0 && t + 2 < n_tiles) issue(t + 2, buf);
-    }
-    // fixed-order block reduction of the round's accumulators
-    round_reduce<NP, MIX>(c, r0, np_, ar, az, fr, fz, kr, kz, sa);
-}
-
-// Adaptive far sum (SPT_FAR_ADAPTIVE) for points r0..r0+np_-1 of the list.
-// Segments are taken kAdaptSegs at a time (32 runs of SPT_BLOCK_SEGS).  One
-// warp classifies the chunk's runs by the smallest lower-bound distance over
-// the round's points: flagged runs at least ratio_run arclengths away take
-// the 8-point rule over the whole run (list R3), runs whose every segment is
-// at least ratio2 lengths away take Gauss-2 on each segment (R2), the rest
-// (M) are classified segment by segment -- below ratio4 lengths the
-// reference nodes, with an 8-bit mask of the points for which the segment is
-// near (they skip it), below ratio2 Gauss-4, else Gauss-2 (lists L0, L1, L2,
-// in the TMA tile region, which this rule does not use).  The flattened node
-// list L0 | L1 | L2 | R2 | R3 is then evaluated like far_round's tiles,
-// nodes read through L1/L2.  Without run bounds every run is in M.
-constexpr int kAdaptSegs = 1024;
-constexpr int kAdaptRuns = kAdaptSegs / SPT_BLOCK_SEGS;
-static_assert(kAdaptRuns == 32, "one warp classifies a chunk's runs");
-static_assert(3 * kAdaptSegs * sizeof(int) <= 2 * 3 * 256 * sizeof(double), "segment lists must fit the smallest tile region");
-static_assert(kAdaptSegs <= kRound * 256, "near masks must fit the near-flag bytes");
-static_assert(160 <= kWarps * 3 * kRound * 2, "run lists and counts fit the reduction scratch");
-
-template <int NP, int NQ, bool MIX>
-__device__ void far_adaptive(Ctx& c, int r0, int np_, unsigned long long& far_evals) {
-    const SptBem& b = c.bem;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nseg = b.n_seg, nps = b.nodes_per_seg;
-    double* P = c.bpt;
-    int* lists = reinterpret_cast<int*>(c.tiles);  // L0 | L1 | L2, kAdaptSegs each
-    unsigned char* mask = c.nflag;                 // near masks of L0
-    // counts and run lists in the reduction scratch (free until the final reduction)
-    int* s_wc = reinterpret_cast<int*>(c.red);     // [3][kWarps] per-warp level counts
-    int* s_n = s_wc + 24;                          // [3] lengths of L0, L1, L2
-    int* s_rn = s_wc + 27;                         // [3] lengths of R2, R3, M
-    int* R2 = s_wc + 32;
-    int* R3 = s_wc + 64;
-    int* M = s_wc + 96;
-    int* Mcls = s_wc + 128;
-    double pr[NP], pinv[NP], pz[NP], ar[NP], az[NP];
-    float fr[NP], fz[NP], kr[NP], kz[NP], prf[NP], pinvf[NP];
-    float sa[NP];
-#pragma unroll
-    for (int p = 0; p < NP; ++p) {
-        const int k = r0 + (p < np_ ? p : 0);
-        pr[p] = P[8 * k + 3];
-        pinv[p] = pr[p] > 0.0 ? 1.0 / pr[p] : 0.0;
-        pz[p] = P[8 * k + 4];
-        ar[p] = 0.0;
-        az[p] = 0.0;
-        fr[p] = fz[p] = kr[p] = kz[p] = sa[p] = 0.0f;
-        prf[p] = (float)pr[p];
-        pinvf[p] = (float)pinv[p];
-    }
-    if (MIX && tid == 0) *c.redo = 0;  // ordered before the reduction's writes by the barriers between
-    const double r4 = b.ratio4, r2 = b.ratio2;
-    const double* cr = b.coarse;
-    const double* cz = b.coarse + b.coarse_stride;
-    const double* cw = b.coarse + 2 * b.coarse_stride;
-    const bool run_rule = b.blk && b.run_nodes && b.ratio_run > 0.0;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int c0 = 0; c0 < nseg; c0 += kAdaptSegs) {
-        const int q0 = c0 / SPT_BLOCK_SEGS;
-        const int nr = min(kAdaptRuns, (nseg - c0 + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS);
-        if (warp == 0) {
-            const int q = q0 + lane;
-            int cls = -1;  // 3 run rule, 2 Gauss-2 on every segment, 1 no near segment, 0 full test
-            if (lane < nr) {
-                cls = 0;
-                if (b.blk) {
-                    double lb = INFINITY;
-                    for (int p = 0; p < np_; ++p) lb = fmin(lb, blk_lower(b, q, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4]));
-                    const double lm = blk_lmax(b, q);
-                    if (run_rule && __ldg(b.blk + 5 * b.blk_stride + q) != 0.0 &&
-                        lb >= b.ratio_run * __ldg(b.blk + 4 * b.blk_stride + q))
-                        cls = 3;
-                    else if (lb >= r2 * lm) cls = 2;
-                    else if (lb >= r4 * lm) cls = 1;
-                }
-            }
-            const unsigned b3 = __ballot_sync(0xffffffffu, cls == 3);
-            const unsigned b2 = __ballot_sync(0xffffffffu, cls == 2);
-            const unsigned bm = __ballot_sync(0xffffffffu, cls == 0 || cls == 1);
-            if (cls == 3) R3[__popc(b3 & lt)] = q;
-            if (cls == 2) R2[__popc(b2 & lt)] = q;
-            if (cls == 0 || cls == 1) { M[__popc(bm & lt)] = q; Mcls[__popc(bm & lt)] = cls; }
-            if (lane == 0) { s_rn[0] = __popc(b2); s_rn[1] = __popc(b3); s_rn[2] = __popc(bm); }
-            if (lane < 3) s_n[lane] = 0;
-        }
-        __syncthreads();
-        // segment classification of the M runs: one run per warp per wave
-        const int nm = s_rn[2];
-        for (int w0 = 0; w0 < nm; w0 += kWarps) {
-            const int mi = w0 + warp;
-            int lvl = 3;
-            unsigned m = 0;
-            int sg = 0;
-            if (mi < nm) {
-                sg = M[mi] * SPT_BLOCK_SEGS + lane;
-                if (sg < nseg) {
-                    const int cls = Mcls[mi];
-                    const double L = segf(b, 4, sg);
-                    double dmin = INFINITY;
-                    for (int p = 0; p < np_; ++p) {
-                        double proj, dist;
-                        if (seg_near(b, sg, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4], proj, dist)) m |= 1u << p;
-                        dmin = fmin(dmin, dist);
-                    }
-                    if (cls == 1) m = 0, lvl = dmin < r2 * L ? 1 : 2;
-                    else lvl = dmin < r4 * L ? 0 : (dmin < r2 * L ? 1 : 2);
-                }
-            }
-            unsigned bal[3];
-#pragma unroll
-            for (int v = 0; v < 3; ++v) {
-                bal[v] = __ballot_sync(0xffffffffu, lvl == v);
-                if (lane == 0) s_wc[v * kWarps + warp] = __popc(bal[v]);
-            }
-            __syncthreads();
-            if (lvl < 3) {
-                int pos = s_n[lvl] + __popc(bal[lvl] & lt);
-                for (int w = 0; w < warp; ++w) pos += s_wc[lvl * kWarps + w];
-                lists[lvl * kAdaptSegs + pos] = sg;
-                if (lvl == 0) mask[pos] = (unsigned char)m;
-            }
-            __syncthreads();
-            if (tid < 3) {
-                int t = 0;
-                for (int w = 0; w < kWarps; ++w) t += s_wc[tid * kWarps + w];
-                s_n[tid] += t;
-            }
-            __syncthreads();
-        }
-        const int e0 = s_n[0] * nps, e1 = e0 + 4 * s_n[1], e2 = e1 + 2 * s_n[2];
-        const int e3 = e2 + 2 * SPT_BLOCK_SEGS * s_rn[0], e4 = e3 + SPT_RUN_NODES * s_rn[1];
-        for (int q0i = tid; q0i < e4; q0i += kThreads * NQ) {
-            double rq[NQ], zq[NQ], wq[NQ];
-            unsigned mk[NQ];
-            bool in[NQ];
-#pragma unroll
-            for (int j = 0; j < NQ; ++j) {
-                const int q = q0i + j * kThreads;
-                in[j] = q < e4;
-                size_t src = 0;
-                const double *tr = cr, *tz = cz, *tw = cw;
-                mk[j] = 0;
-                if (!in[j]) {
-                    // padding lane: any valid node, not accumulated
-                } else if (q < e0) {
-                    const int li = q / nps;
-                    src = (size_t)lists[li] * nps + (q - li * nps);
-                    tr = b.node;
-                    tz = b.node + b.node_stride;
-                    tw = b.node + 2 * b.node_stride;
-                    mk[j] = mask[li];
-                } else if (q < e1) {
-                    const int i = q - e0;
-                    src = (size_t)lists[kAdaptSegs + (i >> 2)] * 6 + (i & 3);
-                } else if (q < e2) {
-                    const int i = q - e1;
-                    src = (size_t)lists[2 * kAdaptSegs + (i >> 1)] * 6 + 4 + (i & 1);
-                } else if (q < e3) {
-                    const int i = q - e2;
-                    const int sgi = R2[i / (2 * SPT_BLOCK_SEGS)] * SPT_BLOCK_SEGS + ((i & (2 * SPT_BLOCK_SEGS - 1)) >> 1);
-                    if (sgi < nseg) src = (size_t)sgi * 6 + 4 + (i & 1);
-                    else in[j] = false;  // past the last segment of a short final run
-                } else {
-                    const int i = q - e3;
-                    src = (size_t)R3[i / SPT_RUN_NODES] * SPT_RUN_NODES + (i % SPT_RUN_NODES);
-                    tr = b.run_nodes;
-                    tz = b.run_nodes + b.run_stride;
-                    tw = b.run_nodes + 2 * b.run_stride;
-                }
-                rq[j] = __ldg(tr + src);
-                zq[j] = __ldg(tz + src);
-                wq[j] = __ldg(tw + src);
-            }
-#pragma unroll
-            for (int p = 0; p < NP; ++p) {
-#pragma unroll
-                for (int j = 0; j < NQ; ++j) {
-                    if (p < np_ && in[j] && !((mk[j] >> p) & 1u)) {
-                        const double dz = pz[p] - zq[j];
-                        if (MIX) {
-                            float er, ez;
-                            if (ring_far_f(prf[p], pinvf[p], (float)(pr[p] - rq[j]), (float)(pr[p] + rq[j]), (float)dz,
-                                           (float)rq[j], er, ez)) {
-                                const float w = (float)wq[j];
-                                kahan_add(fr[p], kr[p], w * er);
-                                kahan_add(fz[p], kz[p], w * ez);
-                                sa[p] += fabsf(w * er) + fabsf(w * ez);
-                            } else {
-                                double e64r, e64z;
-                                ring_field_far(pr[p], pinv[p], dz, rq[j], e64r, e64z);
-                                ar[p] = fma(wq[j], e64r, ar[p]);
-                                az[p] = fma(wq[j], e64z, az[p]);
-                            }
-                        } else {
-                            double er, ez;
-                            ring_field_far(pr[p], pinv[p], dz, rq[j], er, ez);
-                            ar[p] = fma(wq[j], er, ar[p]);
-                            az[p] = fma(wq[j], ez, az[p]);
-                        }
-                        ++far_evals;
-                    }
-                }
-            }
-        }
-        __syncthreads();  // the lists are rewritten by the next chunk
-    }
-    round_reduce<NP, MIX>(c, r0, np_, ar, az, fr, fz, kr, kz, sa);
-}
-
-// ---------------------------------------------------------------------------
-// BEM field of a list of points, in phases.  Records live in c.bpt (8 doubles
-// each: x, y, z, rho_e, z_e, then results); every phase is called by all
-// threads of the CTA.
-
-// A: closest segment and on-surface offset of records [0, n).  With `frame`,
-// also the closest segment, its parameter t and the distance, for the
-// surrogate's inputs.
-__device__ void bem_closest(Ctx& c, int n, bool frame) {
-    const SptBem& b = c.bem;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double* P = c.bpt;  // record k: [0]x [1]y [2]z [3]rho_e [4]z_e [5]ax [6]ay [7]near_r ; near_z in fld tmp
-    const int nseg = b.n_seg;
-
-    // A: closest point + on-surface offset (one warp per point)
-    for (int k = warp; k < n; k += kWarps) {
-        const double x = P[8 * k + 0], y = P[8 * k + 1], z = P[8 * k + 2];
-        const double rho = hypot(x, y);
-        double best = INFINITY;
-        int bs = 0x7fffffff;
-        if (b.blk) {
-            // the run with the smallest lower bound gives an upper bound of the
-            // minimum; only runs whose lower bound does not exceed it are scanned
-            // (each lane still takes its segments in increasing order)
-            const int nblk = (nseg + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS;
-            double lbm = INFINITY;
-            int qm = 0;
-            for (int q = lane; q < nblk; q += 32) {
-                const double lb = blk_lower(b, q, rho, z);
-                if (lb < lbm) { lbm = lb; qm = q; }
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double ol = __shfl_xor_sync(0xffffffffu, lbm, o);
-                const int oq = __shfl_xor_sync(0xffffffffu, qm, o);
-                if (ol < lbm || (ol == lbm && oq < qm)) { lbm = ol; qm = oq; }
-            }
-            double ub = INFINITY;
-            if (qm * SPT_BLOCK_SEGS + lane < nseg) ub = seg_dist2(b, qm * SPT_BLOCK_SEGS + lane, rho, z);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) ub = fmin(ub, __shfl_xor_sync(0xffffffffu, ub, o));
-            const double ubd = sqrt(ub);
-            for (int q0 = 0; q0 < nblk; q0 += 32) {
-                const bool cand = q0 + lane < nblk && !(blk_lower(b, q0 + lane, rho, z) > ubd);
-                unsigned cm = __ballot_sync(0xffffffffu, cand);
-                while (cm) {
-                    const int j = __ffs(cm) - 1;
-                    cm &= cm - 1;
-                    const int s = (q0 + j) * SPT_BLOCK_SEGS + lane;
-                    if (s < nseg) {
-                        const double d2 = seg_dist2(b, s, rho, z);
-                        if (d2 < best) { best = d2; bs = s; }
-                    }
-                }
-            }
-        } else {
-            for (int s = lane; s < nseg; s += 32) {
-                const double d2 = seg_dist2(b, s, rho, z);
-                if (d2 < best) { best = d2; bs = s; }
-            }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-            const int os = __shfl_xor_sync(0xffffffffu, bs, o);
-            if (ob < best || (ob == best && os < bs)) { best = ob; bs = os; }
-        }
-        if (lane == 0) {
-            if (bs >= nseg) bs = 0;  // every distance was NaN: the reference keeps index 0
-            const double Ls = segf(b, 4, bs);
-            const double thr = __dmul_rn(1e-9, Ls);
-            const double off = (best < __dmul_rn(thr, thr)) ? __dmul_rn(1e-4, Ls) : 0.0;
-            double re = __dadd_rn(rho, __dmul_rn(off, segf(b, 7, bs)));
-            if (rho == 0.0) re = 0.0;
-            P[8 * k + 3] = re;
-            P[8 * k + 4] = __dadd_rn(z, __dmul_rn(off, segf(b, 8, bs)));
-            if (frame) {
-                const double p0x = segf(b, 0, bs), p0y = segf(b, 1, bs), ax = segf(b, 2, bs), ay = segf(b, 3, bs);
-                double tt = ((rho - p0x) * ax + (z - p0y) * ay) / (ax * ax + ay * ay);
-                c.sseg[k] = bs;
-                c.st[k] = fmin(fmax(tt, 0.0), 1.0);
-                c.sd[k] = sqrt(best);
-            }
-        }
-    }
-    __syncthreads();
-}
-
-
-// B + C: exact BEM field (E_rho, E_z into record slots 5, 6) of records [0, n)
-// whose slots 3, 4 hold the evaluation point.
-__device__ void bem_sums(Ctx& c, int n, int* status_flag) {
-    const SptBem& b = c.bem;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double* P = c.bpt;
-    const int nseg = b.n_seg;
-    const int nps = b.nodes_per_seg;
-    if (n <= 0) return;
-    // B: near-segment sinh quadrature (one warp per point)
-    unsigned long long n_near = 0, n_ring_near = 0;
-    for (int k = warp; k < n; k += kWarps) {
-        const double re = P[8 * k + 3], ze = P[8 * k + 4];
-        double acc_r = 0.0, acc_z = 0.0;
-        const int nblk = (nseg + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS;
-        for (int q0 = 0; q0 < nblk; q0 += 32) {
-          // runs that may hold a near segment (every run without the bounds table)
-          const bool cand = q0 + lane < nblk && !(b.blk && blk_lower(b, q0 + lane, re, ze) >= blk_lmax(b, q0 + lane));
-          unsigned cm = __ballot_sync(0xffffffffu, cand);
-          while (cm) {
-            const int jq = __ffs(cm) - 1;
-            cm &= cm - 1;
-            const int s0 = (q0 + jq) * SPT_BLOCK_SEGS;
-            const int s = s0 + lane;
-            double proj = 0.0, dist = 0.0;
-            const bool nr = (s < nseg) && seg_near(b, s, re, ze, proj, dist);
-            unsigned mask = __ballot_sync(0xffffffffu, nr);
-            while (mask) {
-                const int j = __ffs(mask) - 1;
-                mask &= mask - 1;
-                const int sg = s0 + j;
-                const double sp = __shfl_sync(0xffffffffu, proj, j);
-                const double Ls = segf(b, 4, sg);
-                const double d = fmax(__shfl_sync(0xffffffffu, dist, j), 1e-15 * Ls);
-                const double lo = asinh(-sp / d), hi = asinh((Ls - sp) / d);
-                const int cnt = max(1, (int)ceil((hi - lo) / 0.5));
-                const double width = (hi - lo) / cnt;
-                const double half = 0.5 * (hi - lo) / cnt;
-                const double p0r = segf(b, 0, sg), p0z = segf(b, 1, sg), ur = segf(b, 5, sg), uz = segf(b, 6, sg);
-                const double sg0 = segf(b, 9, sg), sg1 = segf(b, 10, sg);
-                for (int qn = lane; qn < cnt * 8; qn += 32) {
-                    const int iv = qn >> 3, gi = qn & 7;
-                    const double v = lo + (iv + 0.5 * (b.gauss8_x[gi] + 1.0)) * width;
-                    const double sl = sp + d * sinh(v);
-                    const double sr = p0r + sl * ur, sz = p0z + sl * uz;
-                    const double dens = sg0 + (sl / Ls) * (sg1 - sg0);
-                    const double w = dens * (2.0 * kPi * sr) * d * cosh(v) * half * b.gauss8_w[gi];
-                    double er, ez;
-                    ring_field(re, ze - sz, sr, er, ez);
-                    acc_r += w * er;
-                    acc_z += w * ez;
-                }
-                if (lane == 0) { n_near += 1; n_ring_near += (unsigned long long)cnt * 8; }
-            }
-          }
-        }
-        acc_r = warp_sum(acc_r);
-        acc_z = warp_sum(acc_z);
-        if (lane == 0) {
-            P[8 * k + 7] = acc_r;
-            c.fld[3 * k + 2] = acc_z;  // temporary near_z (fld is rewritten after the far sum)
-        }
-    }
-    if (lane == 0) { c.cnt[SPT_CNT_NEAR_PAIRS] += n_near; c.cnt[SPT_CNT_RING_NEAR] += n_ring_near; }
-    __syncthreads();
-
-    // C: far sum, rounds of up to c.round_pts points over TMA-staged node tiles;
-    // the round's point count selects how many nodes each thread keeps in
-    // flight so that every thread has 8 independent ring evaluations.
-    const int tile_cap = c.L.tile_cap;
-    const int segs_per_tile = min(tile_cap / nps, 256);
-    const int n_tiles = (nseg + segs_per_tile - 1) / segs_per_tile;
-    unsigned long long far_evals = 0;
-    bool ok = true;
-    for (int r0 = 0; r0 < n; r0 += c.round_pts) {
-        const int np_ = min(c.round_pts, n - r0);
-        // mixed form (and the exact sums of the learned form): float32 first,
-        // float64 again for a round whose float32 sums are ill-conditioned
-        bool fp64 = c.form == SPT_FORM_FP64;
-        if (!fp64) {
-            if (b.far_rule == SPT_FAR_ADAPTIVE) {
-                if (np_ == 1) far_adaptive<1, 8, true>(c, r0, np_, far_evals);
-                else if (np_ == 2) far_adaptive<2, 4, true>(c, r0, np_, far_evals);
-                else if (np_ <= 4) far_adaptive<4, 2, true>(c, r0, np_, far_evals);
-                else far_adaptive<8, 1, true>(c, r0, np_, far_evals);
-            } else {
-                if (np_ == 1) far_round<1, 8, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-                else if (np_ == 2) far_round<2, 4, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-                else if (np_ <= 4) far_round<4, 2, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-                else far_round<8, 1, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            }
-            fp64 = *c.redo != 0;
-            // every thread has read the flag before the next round's float32 pass resets it
-            __syncthreads();
-            if (fp64 && tid == 0) ++c.cnt[SPT_CNT_FP64_ROUNDS];
-        }
-        if (!fp64) continue;
-        if (b.far_rule == SPT_FAR_ADAPTIVE) {
-            if (np_ == 1) far_adaptive<1, 8, false>(c, r0, np_, far_evals);
-            else if (np_ == 2) far_adaptive<2, 4, false>(c, r0, np_, far_evals);
-            else if (np_ <= 4) far_adaptive<4, 2, false>(c, r0, np_, far_evals);
-            else far_adaptive<8, 1, false>(c, r0, np_, far_evals);
-        } else {
-            if (np_ == 1)
-                far_round<1, 8, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            else if (np_ == 2)
-                far_round<2, 4, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            else if (np_ <= 4)
-                far_round<4, 2, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            else
-                far_round<8, 1, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-        }
-    }
-    if (!ok && tid == 0) *status_flag = SPT_GROUP_TIMEOUT;
-    c.cnt[SPT_CNT_RING_FAR] += far_evals;
-}
-
-// D: rotate E_rho of records [0, n) into (x, y) (record slots 5, 6, 7 = ex, ey, ez)
-__device__ void bem_rotate(Ctx& c, int n, bool scatter) {
-    const int tid = threadIdx.x;
-    double* P = c.bpt;
-    for (int k = tid; k < n; k += kThreads) {
-        const double x = P[8 * k + 0], y = P[8 * k + 1];
-        const double rho = hypot(x, y);
-        const double e_rho = P[8 * k + 5], e_z = P[8 * k + 6];
-        double ex = 0.0, ey = 0.0;
-        if (rho != 0.0) {
-            ex = e_rho * (x / rho);
-            ey = e_rho * (y / rho);
-        }
-        if (scatter) {
-            const int i = c.list[k];
-            c.fld[3 * i + 0] = ex;
-            c.fld[3 * i + 1] = ey;
-            c.fld[3 * i + 2] = e_z;
-        } else {
-            P[8 * k + 5] = ex;
-            P[8 * k + 6] = ey;
-            P[8 * k + 7] = e_z;
-        }
-    }
-    __syncthreads();
-}
-
-
-// ---------------------------------------------------------------------------
-// learned form: the MLP surrogate evaluated on the tensor cores inside the
-// stage (parameter offsets in the flat parameter array)
-constexpr int kOW1 = 0, kOB1 = 256, kOW2 = 384, kOB2 = 16768, kOW3 = 16896, kOB3 = 33280, kOW4 = 33408, kOB4 = 49792,
-              kOW5 = 49920, kOB5 = 50176;
-
-// Surrogate field (E_rho, E_z) of records [0, n) into c.sout, from the
-// closest-point frame bem_closest(c, n, true) left in sseg/st/sd.  Rows are
-// processed 128 at a time: features and the first layer on the CUDA cores
-// into a BF16 activation tile, three 128 x 128 layers as tcgen05.mma (K = 16
-// steps) into the CTA's TMEM accumulator with the weights streamed into a
-// BF16 tile, bias + SiLU applied while reading TMEM back, the last layer on
-// the CUDA cores, then rescaling and rotation from the (normal, tangent)
-// frame of the closest segment.
-__device__ void mlp_points(Ctx& c, int n, int* status_flag) {
-    const SptBem& b = c.bem;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const float* W = c.sw;
-    const double lmin = log(c.dmin), lspan = log(c.dmax) - lmin;
-    for (int cs = 0; cs < n; cs += 128) {
-        const int m = min(128, n - cs);
-        if (tid < 128) {
-            float u1 = 0.f, u2 = 0.f;
-            if (tid < m) {
-                const int k = cs + tid;
-                const int sg = c.sseg[k];
-                const double sarc = (c.s_start[sg] + c.st[k] * segf(b, 4, sg)) / c.s_end;
-                const double ld = log(fmin(fmax(c.sd[k], c.dmin), c.dmax));
-                u1 = (float)(2.0 * (ld - lmin) / lspan - 1.0);
-                u2 = (float)(2.0 * sarc - 1.0);
-            }
-            c.feat[2 * tid] = u1;
-            c.feat[2 * tid + 1] = u2;
-        }
-        __syncthreads();
-        for (int idx = tid; idx < 128 * 128; idx += kThreads) {
-            const int r = idx >> 7, j = idx & 127;
-            float h = 0.f;
-            if (r < m) {
-                const float v = fmaf(W[kOW1 + 2 * j], c.feat[2 * r], fmaf(W[kOW1 + 2 * j + 1], c.feat[2 * r + 1], W[kOB1 + j]));
-                h = spt_umma::silu(v);
-            }
-            *reinterpret_cast<__nv_bfloat16*>(c.act + spt_umma::kmajor128(r, j)) = __float2bfloat16_rn(h);
-        }
-        for (int l = 0; l < 3; ++l) {
-            const int ow = l == 0 ? kOW2 : (l == 1 ? kOW3 : kOW4);
-            const int ob = l == 0 ? kOB2 : (l == 1 ? kOB3 : kOB4);
-            // weights as the B operand: element (n = out, k = in) at W16[ow + n*128 + k], K-major
-            for (int v = tid; v < 2048; v += kThreads) {
-                const int nrow = v >> 4, kg = v & 15;
-                const uint4 val = *reinterpret_cast<const uint4*>(c.sw16 + ow + nrow * 128 + kg * 8);
-                *reinterpret_cast<uint4*>(c.wt + ((nrow >> 3) * 16 + kg) * 128 + (nrow & 7) * 16) = val;
-            }
-            spt_umma::fence_proxy();
-            __syncthreads();
-            if (tid == 0) {
-                spt_umma::fence_after();
-                const uint32_t idesc = spt_umma::idesc_bf16_128(0, 0);
-#pragma unroll
-                for (int kk = 0; kk < 8; ++kk)
-                    spt_umma::mma(c.tmem, spt_umma::desc(c.act + kk * 256, 128, 2048),
-                                  spt_umma::desc(c.wt + kk * 256, 128, 2048), idesc, kk > 0 ? 1u : 0u);
-                spt_umma::commit(&c.bars[2]);
-            }
-            const bool ok = mbar_wait(&c.bars[2], c.phase[2]);
-            c.phase[2] ^= 1u;
-            if (!ok && tid == 0) *status_flag = SPT_GROUP_TIMEOUT;
-            spt_umma::fence_after();
-            // epilogue: warp w reads TMEM lanes 32 (w % 4) .. +31 (rows), columns 64 (w / 4) .. +63
-            const int row = 32 * (warp & 3) + lane;
-            const int cb = 64 * (warp >> 2);
-#pragma unroll
-            for (int c0 = 0; c0 < 64; c0 += 16) {
-                float v[16];
-                spt_umma::ld16(c.tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(cb + c0), v);
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const int col = cb + c0 + i;
-                    const float h = spt_umma::silu(v[i] + W[ob + col]);
-                    *reinterpret_cast<__nv_bfloat16*>(c.act + spt_umma::kmajor128(row, col)) = __float2bfloat16_rn(h);
-                }
-            }
-            spt_umma::fence_before();
-            spt_umma::fence_proxy();
-            __syncthreads();
-        }
-        // last layer, rescaling and rotation: one warp per row
-        for (int r = warp; r < m; r += kWarps) {
-            float a0 = 0.f, a1 = 0.f;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int j = lane + 32 * q;
-                const float h = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(c.act + spt_umma::kmajor128(r, j)));
-                a0 = fmaf(W[kOW5 + j], h, a0);
-                a1 = fmaf(W[kOW5 + 128 + j], h, a1);
-            }
-            a0 = warp_sum(a0);
-            a1 = warp_sum(a1);
-            if (lane == 0) {
-                const int k = cs + r;
-                const int sg = c.sseg[k];
-                const double t = c.st[k];
-                const double sig = fabs(segf(b, 9, sg) + t * (segf(b, 10, sg) - segf(b, 9, sg))) + c.sig_floor;
-                const double pos = (log(fmin(fmax(c.sd[k], c.dmin), c.dmax)) - lmin) / lspan * 63.0;
-                const int i0 = min(62, max(0, (int)floor(pos)));
-                const double fr = fmin(fmax(pos - i0, 0.0), 1.0);
-                const double g = exp(c.log_scale[i0] + fr * (c.log_scale[i0 + 1] - c.log_scale[i0]));
-                const double en = ((double)a0 + (double)W[kOB5]) * sig * g;
-                const double et = ((double)a1 + (double)W[kOB5 + 1]) * sig * g;
-                c.sout[2 * k] = en * segf(b, 7, sg) + et * segf(b, 5, sg);
-                c.sout[2 * k + 1] = en * segf(b, 8, sg) + et * segf(b, 6, sg);
-            }
-        }
-        __syncthreads();
-    }
-}
-
-__device__ __forceinline__ bool spot_pick(uint32_t key, int particle, double frac) {
-    uint32_t h = key * 0x9E3779B1u ^ (uint32_t)particle * 0x85EBCA77u;
-    h ^= h >> 15;
-    h *= 0x2C1B3C6Du;
-    h ^= h >> 12;
-    return (double)(h & 0xFFFFu) < frac * 65536.0;
-}
-
-// BEM field of the listed points in the learned form: the surrogate for
-// every point, the exact sum for points within the band and for the spot
-// checks (stable partition: exact records first), surrogate error of the
-// spot checks recorded, then the rotation of phase D.
-__device__ void surrogate_points(Ctx& c, int n, int* status_flag) {
-    const int tid = threadIdx.x;
-    double* P = c.bpt;
-    __shared__ int s_cnt[kWarps + 1];
-    __shared__ int s_tot[2];
-    bem_closest(c, n, true);
-    mlp_points(c, n, status_flag);
-    // stable partition of records [0, n): exact (band or spot) first.  The
-    // destination of every record is found first (kept in sseg, which the
-    // MLP no longer needs), then the records move through the act/wt scratch
-    // (8 doubles each: slots 0-4 of the record, the surrogate E_rho, E_z, and
-    // the list entry, negated minus one when the point lies in the band).
-    if (tid == 0) s_tot[0] = 0;
-    __syncthreads();
-    for (int base = 0; base < n; base += kThreads) {
-        const int k = base + tid;
-        const bool ex = k < n && (c.sd[k] < c.band || spot_pick(c.key, c.list[k], c.spot));
-        const unsigned bal = __ballot_sync(0xffffffffu, ex);
-        if ((tid & 31) == 0 && bal) atomicAdd(&s_tot[0], __popc(bal));
-    }
-    __syncthreads();
-    const int ne = s_tot[0];
-    int run_ex = 0, run_su = 0;
-    for (int base = 0; base < n; base += kThreads) {
-        const int k = base + tid;
-        const bool valid = k < n;
-        const bool band = valid && c.sd[k] < c.band;
-        const bool ex = valid && (band || spot_pick(c.key, c.list[k], c.spot));
-        const unsigned be = __ballot_sync(0xffffffffu, ex);
-        if ((tid & 31) == 0) s_cnt[tid >> 5] = __popc(be);
-        __syncthreads();
-        int pre_e = 0, tot_e = 0;
-        for (int w = 0; w < kWarps; ++w) {
-            if (w < (tid >> 5)) pre_e += s_cnt[w];
-            tot_e += s_cnt[w];
-        }
-        const int chunk = min(kThreads, n - base);
-        const int before = min((tid >> 5) * 32, chunk);  // records of this chunk before this warp
-        const unsigned lt = (1u << (tid & 31)) - 1u;
-        if (valid) {
-            const int lane_e = __popc(be & lt);
-            const int dst = ex ? run_ex + pre_e + lane_e : ne + run_su + (before - pre_e) + ((tid & 31) - lane_e);
-            c.sseg[k] = 2 * dst + (band ? 1 : 0);
-        }
-        run_ex += tot_e;
-        run_su += chunk - tot_e;
-        __syncthreads();
-    }
-    double* tmp = reinterpret_cast<double*>(c.act);  // act + wt: 8192 doubles >= 8 n
-    for (int k = tid; k < n; k += kThreads) {
-        const int code = c.sseg[k];
-        const int d = code >> 1;
-        for (int f = 0; f < 5; ++f) tmp[8 * d + f] = P[8 * k + f];
-        tmp[8 * d + 5] = c.sout[2 * k];
-        tmp[8 * d + 6] = c.sout[2 * k + 1];
-        tmp[8 * d + 7] = (code & 1) ? -(double)c.list[k] - 1.0 : (double)c.list[k];
-    }
-    __syncthreads();
-    for (int k = tid; k < n; k += kThreads) {
-        for (int f = 0; f < 5; ++f) P[8 * k + f] = tmp[8 * k + f];
-        c.sout[2 * k] = tmp[8 * k + 5];
-        c.sout[2 * k + 1] = tmp[8 * k + 6];
-        const double v = tmp[8 * k + 7];
-        c.list[k] = v < 0.0 ? (int)(-v - 1.0) : (int)v;
-        c.fld[3 * k] = v < 0.0 ? 1.0 : 0.0;  // band flag, kept where the sums do not write
-    }
-    __syncthreads();
-    bem_sums(c, ne, status_flag);
-    unsigned long long n_spot = 0, n_band = 0;
-    for (int k = tid; k < n; k += kThreads) {
-        if (k >= ne) {
-            P[8 * k + 5] = c.sout[2 * k];
-            P[8 * k + 6] = c.sout[2 * k + 1];
-        } else if (c.fld[3 * k] == 0.0) {  // a spot check: exact and surrogate both known
-            // error relative to the whole external field there (uniform + perturbation)
-            const double er = P[8 * k + 5], ez = P[8 * k + 6];
-            const double dr = c.sout[2 * k] - er, dz = c.sout[2 * k + 1] - ez;
-            const double tz = ez + c.g.E_gun;
-            const float rel = (float)(sqrt(dr * dr + dz * dz) / fmax(sqrt(er * er + tz * tz), 1e-300));
-            if (c.sstats) atomicMax(reinterpret_cast<unsigned int*>(c.sstats) + 6, __float_as_uint(rel));
-            ++n_spot;
-        } else {
-            ++n_band;
-        }
-    }
-    if (c.sstats) {
-        const unsigned long long nsur = (unsigned long long)(n - ne);
-        if (tid == 0 && nsur) atomicAdd(c.sstats + 0, nsur);
-        n_band = warp_sum(n_band);
-        n_spot = warp_sum(n_spot);
-        if ((tid & 31) == 0) {
-            if (n_band) atomicAdd(c.sstats + 1, n_band);
-            if (n_spot) atomicAdd(c.sstats + 2, n_spot);
-        }
-    }
-    __syncthreads();
-    bem_rotate(c, n, false);
-}
-
-// BEM field of the n points listed in c.bpt (x, y, z at slots 0..2 of each
-// 8-double record): the reference's evaluation, phases A-D.
-__device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
-    bem_closest(c, n, false);
-    bem_sums(c, n, status_flag);
-    bem_rotate(c, n, scatter);
-}
-
-// Softened pair sum over the live sources of the group (forces.py:16-29):
-// sum_j k q_i q_j (r_i - r_j) / (|r_i - r_j|^2 + a^2)^1.5, sources given by
-// src(j, x, y, z, q).  float64: the reference's operation order.  Mixed
-// form: separations are taken in float64 (nearby particles far from the
-// origin), then the rest in float32 with Kahan-compensated sums.
-template <bool MIX, typename SRC>
-__device__ __forceinline__ void pair_sum(const Ctx& c, int E, int j0, int jstep, double xi, double yi, double zi,
-                                         double qk, SRC src, double& fx, double& fy, double& fz,
-                                         double* sabs = nullptr) {
-    // sources j0, j0 + jstep, ... (the callers split one target's sources over
-    // the lanes of a warp and add the partial sums)
-    if (!MIX) {
-        double ax = 0.0, ay = 0.0, az = 0.0;
-        for (int j = j0; j < E; j += jstep) {
-            if (!c.live[j]) continue;
-            double x, y, z, q;
-            src(j, x, y, z, q);
-            const double dx = xi - x, dy = yi - y, dz = zi - z;
-            const double r2 = (dx * dx + dy * dy) + dz * dz + c.soft2;
-            const double r3 = r2 * sqrt(r2);
-            const double cf = qk * q / r3;
-            ax = fma(cf, dx, ax);
-            ay = fma(cf, dy, ay);
-            az = fma(cf, dz, az);
-        }
-        fx = ax; fy = ay; fz = az;
-    } else {
-        float ax = 0.f, ay = 0.f, az = 0.f, cx = 0.f, cy = 0.f, cz = 0.f, sa = 0.f;
-        const float soft2 = (float)c.soft2;
-        for (int j = j0; j < E; j += jstep) {
-            if (!c.live[j]) continue;
-            double x, y, z, q;
-            src(j, x, y, z, q);
-            const float dx = (float)(xi - x), dy = (float)(yi - y), dz = (float)(zi - z);
-            const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
-            const float rs = rsqrtf(r2);
-            const float cf = (float)(qk * q) * (rs * rs * rs);
-            kahan_add(ax, cx, cf * dx);
-            kahan_add(ay, cy, cf * dy);
-            kahan_add(az, cz, cf * dz);
-            sa += fabsf(cf * dx) + fabsf(cf * dy) + fabsf(cf * dz);
-        }
-        if (sabs) *sabs += sa;
-        fx = (double)ax - (double)cx;
-        fy = (double)ay - (double)cy;
-        fz = (double)az - (double)cz;
-    }
-}
-
-// sum of v over the T consecutive lanes of a lane group (T a power of two <= 32)
-__device__ __forceinline__ double group_sum(double v, int T) {
-    for (int o = T >> 1; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// ---------------------------------------------------------------------------
-// one stage evaluation for the CTA's group: acc = cm*E + Fc/m + Fimg/m on
-// live particles (geometry.py:289-299).  Positions in c.sp (3E), result in
-// out (3 arrays of stride E... stored as out[0*E+i], out[E+i], out[2E+i]).
-
-template <int KIND>
-__device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
-    const int E = c.E, tid = threadIdx.x;
-    const double* sx = c.sp;
-    const double* sy = c.sp + E;
-    const double* sz = c.sp + 2 * E;
-    const SptGeometry& g = c.g;
-
-    // 1. external field
-    if (KIND == SPT_GEOM_TIP_BEM || KIND == SPT_GEOM_WELL_BEM || KIND == SPT_GEOM_POST_BEM) {
-        // compact the particles that need the BEM sum into c.list (stable order)
-        __shared__ int s_wcount[kWarps + 1];
-        int n_list = 0;
-        for (int base = 0; base < E; base += kThreads) {
-            const int i = base + tid;
-            bool need = false;
-            if (i < E && c.live[i]) {
-                const double x = sx[i], y = sy[i], z = sz[i];
-                need = bem_valid<KIND>(x, y, z, g) && blend_weight(z, g.z_handoff) > 0.0;
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, need);
-            if ((tid & 31) == 0) s_wcount[tid >> 5] = __popc(bal);
-            __syncthreads();
-            if (tid == 0) {
-                int acc = 0;
-                for (int w = 0; w < kWarps; ++w) { const int t = s_wcount[w]; s_wcount[w] = acc; acc += t; }
-                s_wcount[kWarps] = acc;
-            }
-            __syncthreads();
-            if (need) {
-                const int pos = n_list + s_wcount[tid >> 5] + __popc(bal & ((1u << (tid & 31)) - 1u));
-                c.list[pos] = i;
-                c.bpt[8 * pos + 0] = sx[i];
-                c.bpt[8 * pos + 1] = sy[i];
-                c.bpt[8 * pos + 2] = sz[i];
-            }
-            n_list += s_wcount[kWarps];
-            __syncthreads();
-        }
-        if (n_list > 0) {
-            if (c.form == SPT_FORM_SURROGATE)
-                surrogate_points(c, n_list, status_flag);
-            else
-                bem_points(c, n_list, false, status_flag);
-        }
-        // scatter: fld[i] = blended field
-        for (int i = tid; i < E; i += kThreads) { c.fld[3 * i + 0] = 0.0; c.fld[3 * i + 1] = 0.0; c.fld[3 * i + 2] = 0.0; }
-        __syncthreads();
-        for (int k = tid; k < n_list; k += kThreads) {
-            const int i = c.list[k];
-            c.fld[3 * i + 0] = c.bpt[8 * k + 5];
-            c.fld[3 * i + 1] = c.bpt[8 * k + 6];
-            c.fld[3 * i + 2] = c.bpt[8 * k + 7];
-        }
-        __syncthreads();
-    }
-
-    // 2. image sources for the sphere-on-plane construction (forces.py:170-183)
-    const bool three_img = (KIND == SPT_GEOM_TIP || KIND == SPT_GEOM_POST_BEM) && g.has_image;
-    if (three_img) {
-        const double a = g.R - g.z0;
-        const double zc = (KIND == SPT_GEOM_POST_BEM) ? g.L : 0.0;
-        for (int j = tid; j < E; j += kThreads) {
-            const double x = sx[j], y = sy[j], z = sz[j] - zc;
-            const double d = sqrt(x * x + y * y + z * z);
-            const double ds = d > 0.0 ? d : a;
-            const double sh = (a * a) / (ds * ds);
-            c.img[j] = x * sh;
-            c.img[E + j] = y * sh;
-            c.img[2 * E + j] = z * sh;
-            c.img[3 * E + j] = -c.q[j] * (a / ds);
-        }
-        __syncthreads();
-    }
-
-    // 3. per particle: field + pair sums.  Each target's sources are split
-    // over T lanes of a warp (T = 256 / E rounded down to a power of two, at
-    // most 32), whose partial sums are added with shuffles.  Mixed form: the
-    // sums run in float32 first; a target whose sum of |float32 terms| / m
-    // exceeds kappa times its whole acceleration is summed again in float64.
-    int T = 1;
-    while (T < 32 && T * 2 * E <= kThreads) T *= 2;
-    const int per_pass = kThreads / T;
-    const int sub = tid & (T - 1);
-    const int lead = (tid & 31) & ~(T - 1);  // lane of the target's first sub-lane
-    unsigned long long pairs = 0, redone = 0;
-    for (int base = 0; base < E; base += per_pass) {
-        const int i = base + tid / T;
-        const bool act = i < E && c.live[i];
-        const bool mix = c.form != SPT_FORM_FP64;
-        const int ii = i < E ? i : 0;
-        const double xi = sx[ii], yi = sy[ii], zi = sz[ii];
-        const double qk = c.kc * c.q[ii];
-        // this lane's share of the target's Coulomb (fc) and image (fi) sums
-        auto pass = [&](bool f32, bool on, double& fcx, double& fcy, double& fcz, double& fix, double& fiy,
-                        double& fiz, double& sabs) {
-            fcx = fcy = fcz = fix = fiy = fiz = sabs = 0.0;
-            if (!on) return;
-            double* sa = f32 ? &sabs : nullptr;
-            if (E > 1) {
-                auto real = [&](int j, double& x, double& y, double& z, double& q) {
-                    x = sx[j]; y = sy[j]; z = sz[j]; q = c.q[j];
-                };
-                if (f32) pair_sum<true>(c, E, sub, T, xi, yi, zi, qk, real, fcx, fcy, fcz, sa);
-                else pair_sum<false>(c, E, sub, T, xi, yi, zi, qk, real, fcx, fcy, fcz);
-            }
-            if (KIND == SPT_GEOM_FLAT && g.has_image) {
-                const double zimg = -2.0 * g.z0;
-                auto mirror = [&](int j, double& x, double& y, double& z, double& q) {
-                    x = sx[j]; y = sy[j]; z = zimg - sz[j]; q = -c.q[j];
-                };
-                if (f32) pair_sum<true>(c, E, sub, T, xi, yi, zi, qk, mirror, fix, fiy, fiz, sa);
-                else pair_sum<false>(c, E, sub, T, xi, yi, zi, qk, mirror, fix, fiy, fiz);
-            } else if (three_img) {
-                const double zc = (KIND == SPT_GEOM_POST_BEM) ? g.L : 0.0;
-                const double pz0 = (KIND == SPT_GEOM_POST_BEM) ? g.L + g.z0 : g.z0;
-                const double zl = zi - zc;
-                double s1x, s1y, s1z, s2x, s2y, s2z, s3x, s3y, s3z;
-                auto sphere = [&](int j, double& x, double& y, double& z, double& q) {
-                    x = c.img[j]; y = c.img[E + j]; z = c.img[2 * E + j]; q = c.img[3 * E + j];
-                };
-                auto plane = [&](int j, double& x, double& y, double& z, double& q) {
-                    x = sx[j]; y = sy[j]; z = -2.0 * pz0 - (sz[j] - zc); q = -c.q[j];
-                };
-                auto plane_sphere = [&](int j, double& x, double& y, double& z, double& q) {
-                    x = c.img[j]; y = c.img[E + j]; z = -2.0 * pz0 - c.img[2 * E + j]; q = -c.img[3 * E + j];
-                };
-                if (f32) {
-                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, sphere, s1x, s1y, s1z, sa);
-                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, plane, s2x, s2y, s2z, sa);
-                    pair_sum<true>(c, E, sub, T, xi, yi, zl, qk, plane_sphere, s3x, s3y, s3z, sa);
-                } else {
-                    pair_sum<false>(c, E, sub, T, xi, yi, zl, qk, sphere, s1x, s1y, s1z);
-                    pair_sum<false>(c, E, sub, T, xi, yi, zl, qk, plane, s2x, s2y, s2z);
-                    pair_sum<false>(c, E, sub, T, xi, yi, zl, qk, plane_sphere, s3x, s3y, s3z);
-                }
-                fix = (s1x + s2x) + s3x;
-                fiy = (s1y + s2y) + s3y;
-                fiz = (s1z + s2z) + s3z;
-            }
-            // every lane takes part in the shuffles (lanes without work add zeros)
-        };
-        auto reduce = [&](double& fcx, double& fcy, double& fcz, double& fix, double& fiy, double& fiz,
-                          double& sabs) {
-            fcx = group_sum(fcx, T); fcy = group_sum(fcy, T); fcz = group_sum(fcz, T);
-            fix = group_sum(fix, T); fiy = group_sum(fiy, T); fiz = group_sum(fiz, T);
-            sabs = group_sum(sabs, T);
-        };
-        if (act && sub == 0) {
-            pairs += (E > 1 ? E : 0) + ((KIND == SPT_GEOM_FLAT && g.has_image) ? E : 0) + (three_img ? 3 * E : 0);
-        }
-        double fcx, fcy, fcz, fix, fiy, fiz, sabs;
-        pass(mix, act, fcx, fcy, fcz, fix, fiy, fiz, sabs);
-        reduce(fcx, fcy, fcz, fix, fiy, fiz, sabs);
-        double ex = 0.0, ey = 0.0, ez = 0.0;
-        if (act && sub == 0) {
-            if (KIND == SPT_GEOM_FLAT) {
-                ex = 0.0; ey = 0.0; ez = (zi >= 0.0) ? g.E_gun : 0.0;
-            } else if (KIND == SPT_GEOM_TIP) {
-                tip_field(xi, yi, zi, g.E_gun, g.R, ex, ey, ez);
-            } else {
-                // blend(near, far) with near = where(valid, uniform + pert, 0) (bem/geometry.py:44-55, bem/fields.py:186-211)
-                const double w = blend_weight(zi, g.z_handoff);
-                const bool valid = bem_valid<KIND>(xi, yi, zi, g);
-                const double fz = (zi >= 0.0) ? g.E_gun : 0.0;
-                double nx = 0.0, ny = 0.0, nz = 0.0;
-                if (valid && w > 0.0) {
-                    nx = 0.0 + c.fld[3 * i + 0];
-                    ny = 0.0 + c.fld[3 * i + 1];
-                    nz = g.E_gun + c.fld[3 * i + 2];
-                } else if (valid) {
-                    nx = 0.0; ny = 0.0; nz = g.E_gun;  // pert finite; times w = 0
-                }
-                ex = w * nx + (1.0 - w) * 0.0;
-                ey = w * ny + (1.0 - w) * 0.0;
-                ez = w * nz + (1.0 - w) * fz;
-            }
-        }
-        const double mi = act ? c.m[i] : 1.0;
-        auto accel_of = [&](double& ax, double& ay, double& az) {
-            ax = (c.cm * ex + fcx / mi) + fix / mi;
-            ay = (c.cm * ey + fcy / mi) + fiy / mi;
-            az = (c.cm * ez + fcz / mi) + fiz / mi;
-        };
-        double ax = 0.0, ay = 0.0, az = 0.0;
-        bool redo = false;
-        if (act && sub == 0) {
-            accel_of(ax, ay, az);
-            redo = mix && !(sabs / mi <= c.kappa * sqrt(ax * ax + ay * ay + az * az));
-        }
-        redo = __shfl_sync(0xffffffffu, redo, lead);
-        if (__any_sync(0xffffffffu, redo)) {
-            pass(false, act && redo, fcx, fcy, fcz, fix, fiy, fiz, sabs);
-            reduce(fcx, fcy, fcz, fix, fiy, fiz, sabs);
-            if (act && redo && sub == 0) {
-                accel_of(ax, ay, az);
-                ++redone;
-            }
-        }
-        if (i < E && sub == 0) {
-            out[i] = ax;
-            out[E + i] = ay;
-            out[2 * E + i] = az;
-        }
-    }
-    c.cnt[SPT_CNT_FP64_TARGETS] += redone;
-    c.cnt[SPT_CNT_PAIR_EVALS] += pairs;
-    __syncthreads();
-}
-
-// ---------------------------------------------------------------------------
-// flush per-thread counters (all threads call)
-__device__ inline void flush_counters(Ctx& c, unsigned long long* counters) {
-    if (!counters) return;
-    for (int k = 0; k < SPT_N_COUNTERS; ++k) {
-        unsigned long long v = c.cnt[k];
-        v = warp_sum(v);
-        if ((threadIdx.x & 31) == 0 && v) atomicAdd(counters + k, v);
-        c.cnt[k] = 0;
-    }
-}
-
-__device__ inline void init_barriers(Ctx& c) {
-    c.phase[0] = 0u;
-    c.phase[1] = 0u;
-    c.phase[2] = 0u;
-    if (threadIdx.x == 0) {
-        mbar_init(&c.bars[0], 1);
-        mbar_init(&c.bars[1], 1);
-        mbar_init(&c.bars[2], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-}
-
-// ---------------------------------------------------------------------------
-// the persistent integrator
-
-struct GroupScalars {
-    double t, h, hr, next_cp, err, h_next, next_out;
-    int status, exhausted, accepted, out_ptr, out_exh, fire_out;
-    long long n_acc, n_rej;
-};
-
-// number of entries of the ascending array v[0..n) that are <= x
-__device__ __forceinline__ int count_le(const double* v, int n, double x) {
-    int lo = 0, hi = n;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (v[mid] <= x) lo = mid + 1; else hi = mid;
-    }
-    return lo;
-}
-
-// Cubic Hermite pieces (screens.py:118-152), evaluated in the reference's order.
-__device__ __forceinline__ double hermite_z(double p0, double v0, double p1, double v1, double dt, double s) {
-    const double s2 = s * s, s3 = s2 * s;
-    const double h00 = 2 * s3 - 3 * s2 + 1, h10 = s3 - 2 * s2 + s, h01 = -2 * s3 + 3 * s2, h11 = s3 - s2;
-    return h00 * p0 + h10 * dt * v0 + h01 * p1 + h11 * dt * v1;
-}
-
-__device__ __forceinline__ double sgn(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0); }
-
-// Screen crossings of one particle over one accepted step (screens.py:43-115,
-// 155-168): the Hermite z(s) is split at its extrema so each bracket is
-// monotone; a sign change over a bracket is located by 60 bisections and the
-// crossing state (Hermite position and derivative) is appended to the record
-// buffer.  Half-open (t_old, t_new]: a start exactly on the screen is not a crossing.
-__device__ void screen_crossings(const SptTraceParams& prm, const double* o, const double* n, double t_old,
-                                 double dt, long long particle) {
-    const double z0 = o[2], z1 = n[2];
-    bool moving = false;
-    for (int k = 0; k < 6; ++k) moving |= (o[k] != n[k]);
-    if (!moving || !(dt > 0.0)) return;
-    const double u0 = dt * o[5], u1 = dt * n[5];
-    double A = 3 * (2 * (z0 - z1) + u0 + u1);
-    double B = 2 * (3 * (z1 - z0) - 2 * u0 - u1);
-    double C = u0;
-    double sc = fmax(fmax(fabs(A), fabs(B)), fabs(C));
-    sc = sc > 0.0 ? sc : 1.0;
-    A /= sc; B /= sc; C /= sc;
-    const double disc = B * B - 4 * A * C;
-    const double q = -0.5 * (B + (B >= 0.0 ? 1.0 : -1.0) * sqrt(fmax(disc, 0.0)));
-    double r0 = q / (A != 0.0 ? A : 1.0);
-    const double r1 = C / (q != 0.0 ? q : 1.0);
-    const double lin = -C / (B != 0.0 ? B : 1.0);
-    if (A == 0.0) r0 = lin;
-    const bool v0 = (disc >= 0.0) && (A != 0.0 || B != 0.0) && (r0 > 0.0) && (r0 < 1.0);
-    const bool v1 = (disc >= 0.0) && (A != 0.0) && (q != 0.0) && (r1 > 0.0) && (r1 < 1.0);
-    double cut[4] = {0.0, v0 ? r0 : 1.0, v1 ? r1 : 1.0, 1.0};
-    if (cut[1] > cut[2]) { const double tmp = cut[1]; cut[1] = cut[2]; cut[2] = tmp; }
-    for (int sidx = 0; sidx < prm.n_screens; ++sidx) {
-        const double zs = prm.screens[sidx];
-        for (int iv = 0; iv < 3; ++iv) {
-            const double left = cut[iv], right = cut[iv + 1];
-            const double f0 = hermite_z(z0, o[5], z1, n[5], dt, left) - zs;
-            const double f1 = hermite_z(z0, o[5], z1, n[5], dt, right) - zs;
-            if (!(right > left) || f0 == 0.0 || sgn(f0) == sgn(f1)) continue;
-            double lo = left, hi = right, flo = f0;
-            for (int it = 0; it < 60; ++it) {
-                const double mid = 0.5 * (lo + hi);
-                const double fm = hermite_z(z0, o[5], z1, n[5], dt, mid) - zs;
-                const bool same = sgn(fm) == sgn(flo);
-                if (same) { lo = mid; flo = fm; } else { hi = mid; }
-            }
-            const double sv = 0.5 * (lo + hi);
-            const double s2 = sv * sv, s3 = s2 * sv;
-            const double h00 = 2 * s3 - 3 * s2 + 1, h10 = s3 - 2 * s2 + sv, h01 = -2 * s3 + 3 * s2, h11 = s3 - s2;
-            const double d00 = 6 * s2 - 6 * sv, d10 = 3 * s2 - 4 * sv + 1, d01 = -6 * s2 + 6 * sv, d11 = 3 * s2 - 2 * sv;
-            const unsigned long long slot = atomicAdd(prm.screen_count, 1ull);
-            if ((long long)slot >= prm.screen_capacity) continue;
-            const long long cap = prm.screen_capacity;
-            double* r = prm.screen_rec;
-            r[0 * cap + slot] = t_old + sv * dt;
-            for (int k = 0; k < 3; ++k) {
-                r[(1 + k) * cap + slot] = h00 * o[k] + (h10 * dt) * o[3 + k] + h01 * n[k] + (h11 * dt) * n[3 + k];
-                r[(4 + k) * cap + slot] = (d00 / dt) * o[k] + d10 * o[3 + k] + (d01 / dt) * n[k] + d11 * n[3 + k];
-            }
-            r[7 * cap + slot] = (double)sidx;
-            r[8 * cap + slot] = (double)particle;
-        }
-    }
-}
-
-__device__ __forceinline__ void write_output(const SptTraceParams& prm, long long n_particles, int k, long long pidx,
-                                             double t, const double* s) {
-    double* r = prm.output_rec + (size_t)k * 7 * n_particles;
-    r[pidx] = t;
-    for (int c = 0; c < 6; ++c) r[(size_t)(1 + c) * n_particles + pidx] = s[c];
-    prm.output_flag[(size_t)k * n_particles + pidx] = 1;
-}
-
-// learned-form parameters into the context, and the CTA's 128 TMEM columns
-// (the 128 x 128 FP32 accumulator) for its whole lifetime; all threads call
-__device__ void bind_surrogate(Ctx& c, const SptTraceParams& prm, uint32_t* s_tmem) {
-    c.sw = prm.sur_w;
-    c.sw16 = static_cast<const __nv_bfloat16*>(prm.sur_w16);
-    c.s_start = prm.sur_s_start;
-    c.log_scale = prm.sur_log_scale;
-    c.s_end = prm.sur_s_end;
-    c.sig_floor = prm.sur_sig_floor;
-    c.band = prm.sur_band;
-    c.spot = prm.sur_spot;
-    c.dmin = prm.sur_d_min;
-    c.dmax = prm.sur_d_max;
-    c.sstats = prm.sur_stats;
-    if ((threadIdx.x >> 5) == 0) spt_umma::alloc(s_tmem, 128);
-    spt_umma::fence_before();
-    __syncthreads();
-    spt_umma::fence_after();
-    c.tmem = *s_tmem;
-}
-
-__device__ void release_surrogate(Ctx& c) {
-    spt_umma::fence_before();
-    __syncthreads();
-    if ((threadIdx.x >> 5) == 0) spt_umma::dealloc(c.tmem, 128);
-}
-
-template <int KIND>
-__global__ void __launch_bounds__(kThreads, 1)
-trace_kernel(SptState st, SptTraceParams prm, SptGeometry geo, SptBem bem, int* work, double* big_slots) {
-    extern __shared__ __align__(16) double smem[];
-    __shared__ GroupScalars gs;
-    __shared__ int s_g;
-    __shared__ double s_red[kWarps];
-    __shared__ int s_flag;
-    const int tid = threadIdx.x;
-    Ctx c;
-    c.g = geo;
-    c.bem = bem;
-    c.cm = prm.charge_to_mass;
-    c.kc = prm.coulomb_constant;
-    c.soft2 = prm.plummer_radius * prm.plummer_radius;
-    c.form = prm.form;
-    const int Emax = st.max_group_size;
-    const bool sur = prm.form == SPT_FORM_SURROGATE;
-    bind(c, smem, Emax, big_slots ? big_slots + (size_t)blockIdx.x * big_slot_doubles(Emax) : nullptr, sur);
-    // launch-configuration parameters (bind sets the defaults)
-    c.round_pts = (prm.round_points >= 1 && prm.round_points <= kRound) ? prm.round_points : kRound;
-    if (prm.kappa_max > 0.0) c.kappa = prm.kappa_max;
-    __shared__ uint32_t s_tmem;
-    if (sur) bind_surrogate(c, prm, &s_tmem);
-    init_barriers(c);
-
-    // groups to process: all, or the compacted running ones (count written on the device)
-    const int n_run = st.n_active ? *st.n_active : st.n_groups;
-    for (;;) {
-        if (tid == 0) s_g = atomicAdd(work, 1);
-        __syncthreads();
-        const int gi = s_g;
-        __syncthreads();
-        if (gi >= n_run) break;
-        const int g = st.group_order ? st.group_order[gi] : gi;
-        const long long base = st.group_offset[g];
-        const int E = (int)(st.group_offset[g + 1] - base);
-        if (tid == 0) {
-            gs.status = st.status[g];
-            gs.t = st.t[g];
-            gs.h = st.h[g];
-            gs.n_acc = st.n_accepted[g];
-            gs.n_rej = st.n_rejected[g];
-            s_flag = 0;
-        }
-        __syncthreads();
-        if (E <= 0 || gs.status >= SPT_GROUP_DONE) continue;
-        // rebind with this group's size (layout offsets depend on E only through Emax; keep Emax layout)
-        c.E = E;
-        double* y0[6]; double* nw[6];
-        for (int k = 0; k < 6; ++k) { y0[k] = c.y0 + k * Emax; nw[k] = c.nw + k * Emax; }
-        for (int i = tid; i < E; i += kThreads) {
-            y0[0][i] = st.x[base + i]; y0[1][i] = st.y[base + i]; y0[2][i] = st.z[base + i];
-            y0[3][i] = st.vx[base + i]; y0[4][i] = st.vy[base + i]; y0[5][i] = st.vz[base + i];
-            c.tb[i] = st.t_birth[base + i];
-            c.td[i] = st.t_death[base + i];
-            c.q[i] = st.charge[base + i];
-            c.m[i] = st.mass[base + i];
-        }
-        __syncthreads();
-        // sorted birth times (batched_rk45.py:164): rank sort, ties by index
-        for (int i = tid; i < E; i += kThreads) {
-            const double v = c.tb[i];
-            int r = 0;
-            for (int j = 0; j < E; ++j) { const double u = c.tb[j]; r += (u < v) || (u == v && j < i); }
-            c.cps[r] = v;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            gs.fire_out = -1;
-            if (gs.status == SPT_GROUP_NEW) {
-                gs.t = c.cps[0];
-                gs.h = (prm.t_max - gs.t) * prm.initial_step_fraction;
-                // a group born entirely at or after t_max has nothing to integrate: it is
-                // done as it stands (the reference would take a backward step to t_max)
-                gs.status = gs.t < prm.t_max ? SPT_GROUP_RUNNING : SPT_GROUP_DONE;
-                // an output time equal to the start time fires here (batched_rk45.py:191-209)
-                if (prm.n_outputs > 0) {
-                    const int last = count_le(prm.output_times, prm.n_outputs, gs.t) - 1;
-                    if (last >= 0 && prm.output_times[last] == gs.t) gs.fire_out = last;
-                }
-            }
-        }
-        __syncthreads();
-        if (gs.fire_out >= 0) {
-            for (int i = tid; i < E; i += kThreads) {
-                if (c.tb[i] <= gs.t) {
-                    const double sv[6] = {y0[0][i], y0[1][i], y0[2][i], y0[3][i], y0[4][i], y0[5][i]};
-                    write_output(prm, st.n_particles, gs.fire_out, base + i, gs.t, sv);
-                }
-            }
-        }
-        double* kp[7]; double* kv[7];
-        for (int s = 0; s < 7; ++s) { kp[s] = c.kp + 3 * s * Emax; kv[s] = c.kv + 3 * s * Emax; }
-        // The stage routines index slope arrays as out[comp*E + i] with the group's E.
-        for (long long att = 0; att < prm.max_attempts; ++att) {
-            if (gs.status != SPT_GROUP_RUNNING) break;
-            if (tid == 0) {
-                // next checkpoint (batched_rk45.py:228-242)
-                int lo = 0, hi = E;
-                while (lo < hi) { const int mid = (lo + hi) >> 1; if (c.cps[mid] <= gs.t) lo = mid + 1; else hi = mid; }
-                gs.exhausted = lo >= E;
-                gs.next_cp = gs.exhausted ? prm.t_max : c.cps[lo];
-                double target = fmin(gs.next_cp, prm.t_max);
-                if (prm.n_outputs > 0) {
-                    const int optr = count_le(prm.output_times, prm.n_outputs, gs.t);
-                    gs.out_ptr = optr;
-                    gs.out_exh = optr >= prm.n_outputs;
-                    gs.next_out = gs.out_exh ? prm.t_max : prm.output_times[optr];
-                    target = fmin(target, gs.next_out);
-                }
-                gs.hr = fmin(gs.h, target - gs.t);
-                if (!(gs.hr > 0.0) || !isfinite(gs.hr)) gs.status = SPT_GROUP_NONFINITE;
-            }
-            __syncthreads();
-            if (gs.status != SPT_GROUP_RUNNING) break;
-            const double t = gs.t, hr = gs.hr;
-            for (int i = tid; i < E; i += kThreads) c.live[i] = (t >= c.tb[i]) && (t < c.td[i]);
-            __syncthreads();
-            for (int s = 0; s < 6; ++s) {
-                for (int i = tid; i < E; i += kThreads) {
-                    double p[6];
-                    for (int k = 0; k < 6; ++k) p[k] = y0[k][i];
-                    for (int j = 0; j < s; ++j) {
-                        const double a = kA[s][j];
-                        if (a == 0.0) continue;
-                        const double ha = __dmul_rn(hr, a);
-                        for (int k = 0; k < 3; ++k) {
-                            p[k] = __dadd_rn(p[k], __dmul_rn(ha, kp[j][k * E + i]));
-                            p[3 + k] = __dadd_rn(p[3 + k], __dmul_rn(ha, kv[j][k * E + i]));
-                        }
-                    }
-                    const bool lv = c.live[i];
-                    for (int k = 0; k < 3; ++k) {
-                        c.sp[k * E + i] = p[k];
-                        kp[s][k * E + i] = lv ? p[3 + k] : 0.0;
-                    }
-                }
-                __syncthreads();
-                c.key = (uint32_t)g * 2654435761u ^ (uint32_t)(gs.n_acc + gs.n_rej) * 40503u ^ (uint32_t)s * 97u;
-                stage_accel<KIND>(c, kv[s], &s_flag);
-            }
-            // 5th-order solution and the endpoint stage (batched_rk45.py:365-370)
-            for (int i = tid; i < E; i += kThreads) {
-                for (int k = 0; k < 3; ++k) {
-                    double sp = 0.0, sv = 0.0;
-                    for (int j = 0; j < 6; ++j) {
-                        sp = __dadd_rn(sp, __dmul_rn(kB[j], kp[j][k * E + i]));
-                        sv = __dadd_rn(sv, __dmul_rn(kB[j], kv[j][k * E + i]));
-                    }
-                    const double pn = __dadd_rn(y0[k][i], __dmul_rn(hr, sp));
-                    const double vn = __dadd_rn(y0[3 + k][i], __dmul_rn(hr, sv));
-                    nw[k][i] = pn;
-                    nw[3 + k][i] = vn;
-                    c.sp[k * E + i] = pn;
-                    kp[6][k * E + i] = c.live[i] ? vn : 0.0;
-                }
-            }
-            __syncthreads();
-            c.key = (uint32_t)g * 2654435761u ^ (uint32_t)(gs.n_acc + gs.n_rej) * 40503u ^ 6u * 97u;
-            stage_accel<KIND>(c, kv[6], &s_flag);
-            // embedded error norm (batched_rk45.py:372-393)
-            double part = 0.0;
-            for (int i = tid; i < E; i += kThreads) {
-                for (int k = 0; k < 3; ++k) {
-                    double ep = 0.0, ev = 0.0;
-                    for (int j = 0; j < 7; ++j) {
-                        ep = __dadd_rn(ep, __dmul_rn(kE[j], kp[j][k * E + i]));
-                        ev = __dadd_rn(ev, __dmul_rn(kE[j], kv[j][k * E + i]));
-                    }
-                    ep = __dmul_rn(hr, ep);
-                    ev = __dmul_rn(hr, ev);
-                    const double scp = __dadd_rn(prm.atol, __dmul_rn(prm.rtol, fmax(fabs(y0[k][i]), fabs(nw[k][i]))));
-                    const double scv = __dadd_rn(kSpeedOfLight * prm.atol,
-                                                 __dmul_rn(prm.rtol, fmax(fabs(y0[3 + k][i]), fabs(nw[3 + k][i]))));
-                    const double a = __ddiv_rn(ep, scp), b = __ddiv_rn(ev, scv);
-                    part = __dadd_rn(part, __dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
-                }
-            }
-            part = warp_sum(part);
-            if ((tid & 31) == 0) s_red[tid >> 5] = part;
-            __syncthreads();
-            if (tid == 0) {
-                double sq = 0.0;
-                for (int w = 0; w < kWarps; ++w) sq += s_red[w];
-                double err = sqrt(sq / (double)(6 * E));
-                if (err == 0.0) err = kTiny;
-                const bool acc = err <= 1.0;
-                double fac = prm.safety * pow(err, -1.0 / 5.0);
-                fac = fmin(fmax(fac, prm.min_factor), prm.max_factor);
-                gs.err = err;
-                gs.accepted = acc;
-                gs.h_next = hr * fac;
-                const long long k_att = gs.n_acc + gs.n_rej;
-                if (prm.log_capacity > 0 && k_att < prm.log_capacity) {
-                    prm.log_h[(size_t)g * prm.log_capacity + k_att] = hr;
-                    prm.log_err[(size_t)g * prm.log_capacity + k_att] = err;
-                }
-                c.cnt[SPT_CNT_ATTEMPTS] += 1;
-                c.cnt[SPT_CNT_STAGE_EVALS] += 7ull * E;
-            }
-            __syncthreads();
-            if (gs.accepted) {
-                const double t_new = t + hr;
-                const double dt = t_new - t;
-                const double tol_out = 1e-9 * fmax(prm.t_max, 1e-30);
-                const bool hit = prm.n_outputs > 0 && !gs.out_exh && t_new >= gs.next_out - tol_out;
-                for (int i = tid; i < E; i += kThreads) {
-                    const bool was = c.live[i];
-                    if (was && kill_test<KIND>(nw[0][i], nw[1][i], nw[2][i], geo)) c.td[i] = t_new;
-                    double o[6], nv[6];
-                    for (int k = 0; k < 6; ++k) { o[k] = y0[k][i]; nv[k] = nw[k][i]; }
-                    if (hit && c.tb[i] <= t_new) write_output(prm, st.n_particles, gs.out_ptr, base + i, t_new, nv);
-                    if (prm.n_screens > 0) screen_crossings(prm, o, nv, t, dt, base + i);
-                    for (int k = 0; k < 6; ++k) y0[k][i] = nv[k];
-                }
-                if (tid == 0) {
-                    gs.t = t_new;
-                    gs.n_acc += 1;
-                    const double tol = 1e-9 * fmax(prm.t_max, 1e-30);
-                    if (!gs.exhausted && t_new >= gs.next_cp - tol)
-                        gs.h = (prm.t_max - t_new) * prm.initial_step_fraction;
-                    else
-                        gs.h = gs.h_next;
-                    if (!(t_new < prm.t_max * (1 - 1e-14))) gs.status = SPT_GROUP_DONE;
-                    c.cnt[SPT_CNT_ACCEPTED] += 1;
-                    c.cnt[SPT_CNT_PARTICLE_STEPS] += (unsigned long long)E;
-                }
-            } else if (tid == 0) {
-                gs.h = gs.h_next;
-                gs.n_rej += 1;
-            }
-            if (tid == 0) {
-                if (isnan(gs.err)) gs.status = SPT_GROUP_NONFINITE;
-                if (s_flag) gs.status = s_flag;
-            }
-            __syncthreads();
-        }
-        // write back
-        for (int i = tid; i < E; i += kThreads) {
-            st.x[base + i] = y0[0][i]; st.y[base + i] = y0[1][i]; st.z[base + i] = y0[2][i];
-            st.vx[base + i] = y0[3][i]; st.vy[base + i] = y0[4][i]; st.vz[base + i] = y0[5][i];
-            st.t_death[base + i] = c.td[i];
-        }
-        if (tid == 0) {
-            st.t[g] = gs.t;
-            st.h[g] = gs.h;
-            st.status[g] = gs.status;
-            st.n_accepted[g] = gs.n_acc;
-            st.n_rejected[g] = gs.n_rej;
-        }
-        flush_counters(c, prm.counters);
-        __syncthreads();
-        // A timed-out barrier wait leaves this CTA's barrier phases unknown:
-        // stop taking groups (the remaining ones stay NEW/RUNNING for the host).
-        if (s_flag == SPT_GROUP_TIMEOUT) break;
-    }
-    if (sur) release_surrogate(c);
-}
-
-// one stage evaluation per group (spt_accel)
-template <int KIND>
-__global__ void __launch_bounds__(kThreads, 1)
-accel_kernel(SptAccelArgs a, SptGeometry geo, SptBem bem) {
-    extern __shared__ __align__(16) double smem[];
-    __shared__ int s_flag;
-    const int tid = threadIdx.x;
-    const int g = blockIdx.x;
-    Ctx c;
-    c.g = geo;
-    c.bem = bem;
-    c.cm = a.charge_to_mass;
-    c.kc = a.coulomb_constant;
-    c.soft2 = a.plummer_radius * a.plummer_radius;
-    c.form = a.form;
-    const int Emax = a.max_group_size;
-    // the accel path keeps no slopes: bind a layout without the big-slot region
-    bind(c, smem, Emax, nullptr);
-    init_barriers(c);
-    const long long base = a.group_offset[g];
-    const int E = (int)(a.group_offset[g + 1] - base);
-    c.E = E;
-    if (tid == 0) s_flag = 0;
-    for (int i = tid; i < E; i += kThreads) {
-        c.sp[i] = a.x[base + i];
-        c.sp[E + i] = a.y[base + i];
-        c.sp[2 * E + i] = a.z[base + i];
-        c.live[i] = a.active[base + i];
-        c.q[i] = a.charge[base + i];
-        c.m[i] = a.mass[base + i];
-    }
-    __syncthreads();
-    double* out = c.kv;  // slope storage is free on this path (groups here are at most kSmallGroup)
-    stage_accel<KIND>(c, out, &s_flag);
-    for (int i = tid; i < E; i += kThreads) {
-        a.ax[base + i] = out[i];
-        a.ay[base + i] = out[E + i];
-        a.az[base + i] = out[2 * E + i];
-    }
-}
+SPT_DECLARE_KIND(SPT_GEOM_FLAT)
+SPT_DECLARE_KIND(SPT_GEOM_TIP)
+SPT_DECLARE_KIND(SPT_GEOM_TIP_BEM)
+SPT_DECLARE_KIND(SPT_GEOM_WELL_BEM)
+SPT_DECLARE_KIND(SPT_GEOM_POST_BEM)
 
 // BEM perturbation field at arbitrary points (spt_bem_field): kRound*8 points per CTA
 constexpr int kFieldChunk = 64;
-__global__ void __launch_bounds__(kThreads, 1)
-bem_field_kernel(const double* x, const double* y, const double* z, long long n, SptBem bem, int form, double* ex,
-                 double* ey, double* ez, unsigned long long* counters) {
+template <int FORM, int FAR>
+__global__ void __launch_bounds__(kMaxThreads, 1)
+bem_field_kernel(const double* x, const double* y, const double* z, long long n, const __grid_constant__ SptBem bem,
+                 double* ex, double* ey, double* ez, unsigned long long* counters) {
     extern __shared__ __align__(16) double smem[];
     __shared__ int s_flag;
-    Ctx c;
-    c.g = SptGeometry{};
-    c.bem = bem;
-    c.form = form;
-    bind(c, smem, kFieldChunk, nullptr);
+    __shared__ unsigned long long s_cnt[SPT_N_COUNTERS];
+    __shared__ SptGeometry s_geo;
+    if (threadIdx.x == 0) s_geo = SptGeometry{};
+    __syncthreads();
+    Ctx c(s_geo, bem);
+    bind(c, smem, kFieldChunk, FAR, nullptr, s_cnt);
     init_barriers(c);
     const long long p0 = (long long)blockIdx.x * kFieldChunk;
     const int np_ = (int)min((long long)kFieldChunk, n - p0);
-    for (int k = threadIdx.x; k < np_; k += kThreads) {
+    for (int k = threadIdx.x; k < np_; k += c.nt) {
         c.bpt[8 * k + 0] = x[p0 + k];
         c.bpt[8 * k + 1] = y[p0 + k];
         c.bpt[8 * k + 2] = z[p0 + k];
     }
     if (threadIdx.x == 0) s_flag = 0;
     __syncthreads();
-    bem_points(c, np_, false, &s_flag);
-    for (int k = threadIdx.x; k < np_; k += kThreads) {
+    bem_points<FORM, FAR>(c, np_, false, &s_flag);
+    for (int k = threadIdx.x; k < np_; k += c.nt) {
         ex[p0 + k] = c.bpt[8 * k + 5];
         ey[p0 + k] = c.bpt[8 * k + 6];
         ez[p0 + k] = c.bpt[8 * k + 7];
     }
+    __syncthreads();
     flush_counters(c, counters);
 }
 
 // learned-form field at arbitrary points (spt_surrogate_field): 128 points
 // (one MLP tile) per CTA, through the stage kernel's surrogate_points
 constexpr int kSurChunk = 128;
-__global__ void __launch_bounds__(kThreads, 1)
-surrogate_field_kernel(const double* x, const double* y, const double* z, long long n, SptBem bem, SptTraceParams prm,
-                       double* ex, double* ey, double* ez, unsigned long long* counters) {
+template <int FAR>
+__global__ void __launch_bounds__(kMaxThreads, 1)
+surrogate_field_kernel(const double* x, const double* y, const double* z, long long n,
+                       const __grid_constant__ SptBem bem, const __grid_constant__ SptTraceParams prm, double* ex,
+                       double* ey, double* ez, unsigned long long* counters) {
     extern __shared__ __align__(16) double smem[];
     __shared__ int s_flag;
     __shared__ uint32_t s_tmem;
-    Ctx c;
-    c.g = SptGeometry{};
-    c.bem = bem;
-    c.form = SPT_FORM_SURROGATE;
-    bind(c, smem, kSurChunk, nullptr, true);
+    __shared__ unsigned long long s_cnt[SPT_N_COUNTERS];
+    __shared__ SptGeometry s_geo;
+    if (threadIdx.x == 0) s_geo = SptGeometry{};
+    __syncthreads();
+    Ctx c(s_geo, bem);
+    bind(c, smem, kSurChunk, FAR, nullptr, s_cnt, true);
     bind_surrogate(c, prm, &s_tmem);
     init_barriers(c);
     c.key = 0x2545F491u;
     const long long p0 = (long long)blockIdx.x * kSurChunk;
     const int np_ = (int)min((long long)kSurChunk, n - p0);
-    for (int k = threadIdx.x; k < np_; k += kThreads) {
+    for (int k = threadIdx.x; k < np_; k += c.nt) {
         c.bpt[8 * k + 0] = x[p0 + k];
         c.bpt[8 * k + 1] = y[p0 + k];
         c.bpt[8 * k + 2] = z[p0 + k];
@@ -2005,14 +93,15 @@ surrogate_field_kernel(const double* x, const double* y, const double* z, long l
     }
     if (threadIdx.x == 0) s_flag = 0;
     __syncthreads();
-    surrogate_points(c, np_, &s_flag);
+    surrogate_points<FAR>(c, np_, &s_flag);
     // records were reordered (exact ones first): c.list holds each one's point index
-    for (int k = threadIdx.x; k < np_; k += kThreads) {
+    for (int k = threadIdx.x; k < np_; k += c.nt) {
         const long long i = c.list[k];
         ex[i] = c.bpt[8 * k + 5];
         ey[i] = c.bpt[8 * k + 6];
         ez[i] = c.bpt[8 * k + 7];
     }
+    __syncthreads();
     flush_counters(c, counters);
     release_surrogate(c);
 }
@@ -2211,36 +300,76 @@ int set_smem(K kernel, size_t bytes) {
                       "cudaFuncSetAttribute");
 }
 
-int grid_for(int n_groups, int blocks_per_sm_hint) {
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const long long cap = (long long)sms * blocks_per_sm_hint;
-    return (int)(n_groups < cap ? n_groups : cap);
+int far_rule_of(const SptGeometry* g, const SptBem* b) { return is_bem(g->kind) && b ? b->far_rule : SPT_FAR_REFERENCE; }
+
+// CTA width of a trace launch: SptTraceParams.cta_threads when it is 32, 64,
+// 128 or 256, else by group size (narrow CTAs for small groups: more groups
+// per SM, fewer warps behind each barrier).  The reference far rule streams
+// 96 KiB node tiles per CTA, so it keeps 256 threads; the learned form needs
+// at least 4 warps (one per 32 TMEM lanes of its 128-row accumulator).
+int trace_threads(const SptState* s, const SptTraceParams* p, int far) {
+    const int want = p->cta_threads;
+    int t;
+    if (want == 32 || want == 64 || want == 128 || want == 256)
+        t = want;
+    else if (far == SPT_FAR_REFERENCE || s->max_group_size > 64)
+        t = 256;
+    else
+        t = s->max_group_size > 16 ? 128 : 64;
+    if (p->form == SPT_FORM_SURROGATE && t < 128) t = 128;
+    return t;
 }
 
-template <int KIND>
-int launch_trace(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b, void* ws,
-                 int64_t ws_bytes, cudaStream_t stream) {
-    const spt::Layout L = spt::make_layout(s->max_group_size, true, p->form == SPT_FORM_SURROGATE);
-    auto kern = spt::trace_kernel<KIND>;
-    int rc = set_smem(kern, L.bytes);
+int dispatch_kind(int kind, const spt::TraceLaunch& t, int form, int far, bool launch, int* grid, size_t* smem,
+                  int* per_sm) {
+    switch (kind) {
+        case SPT_GEOM_FLAT: return spt::trace_dispatch<SPT_GEOM_FLAT>(t, form, far, launch, grid, smem, per_sm);
+        case SPT_GEOM_TIP: return spt::trace_dispatch<SPT_GEOM_TIP>(t, form, far, launch, grid, smem, per_sm);
+        case SPT_GEOM_TIP_BEM: return spt::trace_dispatch<SPT_GEOM_TIP_BEM>(t, form, far, launch, grid, smem, per_sm);
+        case SPT_GEOM_WELL_BEM: return spt::trace_dispatch<SPT_GEOM_WELL_BEM>(t, form, far, launch, grid, smem, per_sm);
+        case SPT_GEOM_POST_BEM: return spt::trace_dispatch<SPT_GEOM_POST_BEM>(t, form, far, launch, grid, smem, per_sm);
+        default: return -1;
+    }
+}
+
+// One trace launch with scratch at `scratch`: the work-queue counter in its
+// first 256 bytes, then (groups above 256 particles) per-CTA slope buffers,
+// scratch_bytes in all; the persistent grid is capped by the buffers it holds
+// and by SptTraceParams.max_ctas.
+int run_trace(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b,
+              unsigned char* scratch, int64_t scratch_bytes, cudaStream_t stream, const char* who) {
+    const int far = far_rule_of(g, b);
+    const spt::Layout L = spt::make_layout(s->max_group_size, far, p->form == SPT_FORM_SURROGATE);
+    spt::TraceLaunch t{};
+    t.s = s;
+    t.p = p;
+    t.g = g;
+    t.bem = b ? *b : SptBem{};
+    t.threads = trace_threads(s, p, far);
+    t.work = reinterpret_cast<int*>(scratch);
+    t.stream = stream;
+    if (L.big) {
+        const int64_t slot_bytes = (int64_t)spt::big_slot_doubles(s->max_group_size) * 8;
+        t.max_slots = (scratch_bytes - 256) / slot_bytes;
+        if (t.max_slots < 1)
+            return fail(SPT_ERR_ARG, "%s: scratch of %lld bytes holds no slope buffer of %lld bytes", who,
+                        (long long)scratch_bytes, (long long)slot_bytes);
+        t.slots = reinterpret_cast<double*>(scratch + 256);
+    }
+    if (p->max_ctas > 0 && (t.max_slots == 0 || t.max_slots > p->max_ctas)) t.max_slots = p->max_ctas;
+    int grid = 0, per_sm = 0;
+    size_t smem = 0;
+    int rc = dispatch_kind(g->kind, t, p->form, far, false, &grid, &smem, &per_sm);
+    if (rc == -1) return fail(SPT_ERR_ARG, "%s: form %d with far rule %d is not offered for geometry kind %d", who, p->form,
+                              far, g->kind);
+    if (rc) return fail(SPT_ERR_CUDA, "%s: launch setup: %s", who, cudaGetErrorString((cudaError_t)rc));
+    if (per_sm < 1) return fail(SPT_ERR_CAPACITY, "%s: group size %d does not fit one CTA", who, s->max_group_size);
+    // the counter must start at zero; the slot buffers are written before they are read
+    rc = cuda_check(cudaMemsetAsync(t.work, 0, sizeof(int), stream), "cudaMemsetAsync");
     if (rc) return rc;
-    int per_sm = 0;
-    rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, spt::kThreads, L.bytes), "occupancy");
-    if (rc) return rc;
-    if (per_sm < 1) return fail(SPT_ERR_CAPACITY, "group size %d does not fit one CTA", s->max_group_size);
-    const int grid = grid_for(s->n_groups, per_sm);
-    int* work = static_cast<int*>(ws);
-    double* slots = nullptr;
-    if (L.big) slots = reinterpret_cast<double*>(static_cast<char*>(ws) + 256);
-    const int64_t need = 256 + (L.big ? (int64_t)grid * (int64_t)spt::big_slot_doubles(s->max_group_size) * 8 : 0);
-    if (ws_bytes < need) return fail(SPT_ERR_ARG, "workspace too small: %lld < %lld", (long long)ws_bytes, (long long)need);
-    rc = cuda_check(cudaMemsetAsync(work, 0, sizeof(int), stream), "cudaMemsetAsync");
-    if (rc) return rc;
-    SptBem bem = b ? *b : SptBem{};
-    kern<<<grid, spt::kThreads, L.bytes, stream>>>(*s, *p, *g, bem, work, slots);
-    return cuda_check(cudaGetLastError(), "trace_kernel launch");
+    rc = dispatch_kind(g->kind, t, p->form, far, true, &grid, &smem, &per_sm);
+    if (rc) return fail(SPT_ERR_CUDA, "%s: trace_kernel launch: %s", who, cudaGetErrorString((cudaError_t)rc));
+    return SPT_OK;
 }
 
 }  // namespace
@@ -2260,12 +389,12 @@ int spt_last_error(char* buf, int32_t len) {
 
 int spt_trace_workspace_bytes(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b,
                               int64_t* bytes) {
-    (void)p; (void)g; (void)b;
-    if (!s || !bytes) return fail(SPT_ERR_ARG, "null argument");
-    const spt::Layout L = spt::make_layout(s->max_group_size, true);
+    if (!s || !p || !g || !bytes) return fail(SPT_ERR_ARG, "null argument");
+    const spt::Layout L = spt::make_layout(s->max_group_size, far_rule_of(g, b), p->form == SPT_FORM_SURROGATE);
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int64_t n = 256;
+    // groups above 256 particles: one slope buffer per CTA, two 256-thread CTAs per SM
     if (L.big) n += (int64_t)sms * 2 * (int64_t)spt::big_slot_doubles(s->max_group_size) * 8;
     *bytes = n;
     return SPT_OK;
@@ -2289,15 +418,8 @@ int spt_trace(const SptState* s, const SptTraceParams* p, const SptGeometry* g, 
         const int rc = check_surrogate(p, g);
         if (rc) return rc;
     }
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    switch (g->kind) {
-        case SPT_GEOM_FLAT: return launch_trace<SPT_GEOM_FLAT>(s, p, g, b, ws, ws_bytes, st);
-        case SPT_GEOM_TIP: return launch_trace<SPT_GEOM_TIP>(s, p, g, b, ws, ws_bytes, st);
-        case SPT_GEOM_TIP_BEM: return launch_trace<SPT_GEOM_TIP_BEM>(s, p, g, b, ws, ws_bytes, st);
-        case SPT_GEOM_WELL_BEM: return launch_trace<SPT_GEOM_WELL_BEM>(s, p, g, b, ws, ws_bytes, st);
-        case SPT_GEOM_POST_BEM: return launch_trace<SPT_GEOM_POST_BEM>(s, p, g, b, ws, ws_bytes, st);
-        default: return fail(SPT_ERR_ARG, "unknown geometry kind %d", g->kind);
-    }
+    return run_trace(s, p, g, b, static_cast<unsigned char*>(ws), ws_bytes, static_cast<cudaStream_t>(stream),
+                     "spt_trace");
 }
 
 int spt_accel(const SptAccelArgs* a, const SptGeometry* g, const SptBem* b, void* stream) {
@@ -2310,26 +432,20 @@ int spt_accel(const SptAccelArgs* a, const SptGeometry* g, const SptBem* b, void
         const int rc = check_bem(b);
         if (rc) return rc;
     }
-    int rc = SPT_OK;
-    const spt::Layout L = spt::make_layout(a->max_group_size, true);
     SptBem bem = b ? *b : SptBem{};
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-#define SPT_LAUNCH_ACCEL(K)                                                                  \
-    {                                                                                        \
-        rc = set_smem(spt::accel_kernel<K>, L.bytes);                                         \
-        if (rc) return rc;                                                                   \
-        spt::accel_kernel<K><<<a->n_groups, spt::kThreads, L.bytes, st>>>(*a, *g, bem);       \
-        return cuda_check(cudaGetLastError(), "accel_kernel launch");                       \
-    }
+    int rc = -1;
     switch (g->kind) {
-        case SPT_GEOM_FLAT: SPT_LAUNCH_ACCEL(SPT_GEOM_FLAT)
-        case SPT_GEOM_TIP: SPT_LAUNCH_ACCEL(SPT_GEOM_TIP)
-        case SPT_GEOM_TIP_BEM: SPT_LAUNCH_ACCEL(SPT_GEOM_TIP_BEM)
-        case SPT_GEOM_WELL_BEM: SPT_LAUNCH_ACCEL(SPT_GEOM_WELL_BEM)
-        case SPT_GEOM_POST_BEM: SPT_LAUNCH_ACCEL(SPT_GEOM_POST_BEM)
+        case SPT_GEOM_FLAT: rc = spt::accel_dispatch<SPT_GEOM_FLAT>(a, g, bem, st); break;
+        case SPT_GEOM_TIP: rc = spt::accel_dispatch<SPT_GEOM_TIP>(a, g, bem, st); break;
+        case SPT_GEOM_TIP_BEM: rc = spt::accel_dispatch<SPT_GEOM_TIP_BEM>(a, g, bem, st); break;
+        case SPT_GEOM_WELL_BEM: rc = spt::accel_dispatch<SPT_GEOM_WELL_BEM>(a, g, bem, st); break;
+        case SPT_GEOM_POST_BEM: rc = spt::accel_dispatch<SPT_GEOM_POST_BEM>(a, g, bem, st); break;
         default: return fail(SPT_ERR_ARG, "unknown geometry kind %d", g->kind);
     }
-#undef SPT_LAUNCH_ACCEL
+    if (rc == -1) return fail(SPT_ERR_ARG, "spt_accel: form %d is not offered here", a->form);
+    if (rc) return fail(SPT_ERR_CUDA, "accel_kernel launch: %s", cudaGetErrorString((cudaError_t)rc));
+    return SPT_OK;
 }
 
 int spt_bem_field(const double* x, const double* y, const double* z, int64_t n, const SptBem* b, int32_t form,
@@ -2339,14 +455,24 @@ int spt_bem_field(const double* x, const double* y, const double* z, int64_t n, 
     int rc = check_bem(b);
     if (rc) return rc;
     if (form != SPT_FORM_FP64 && form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "unknown form %d", form);
-    const spt::Layout L = spt::make_layout(spt::kFieldChunk, true);
-    rc = set_smem(spt::bem_field_kernel, L.bytes);
-    if (rc) return rc;
     const long long blocks = (n + spt::kFieldChunk - 1) / spt::kFieldChunk;
     if (blocks > 0x7fffffffLL) return fail(SPT_ERR_CAPACITY, "too many points");
-    spt::bem_field_kernel<<<(unsigned)blocks, spt::kThreads, L.bytes, static_cast<cudaStream_t>(stream)>>>(
-        x, y, z, n, *b, form, ex, ey, ez, nullptr);
-    return cuda_check(cudaGetLastError(), "bem_field_kernel launch");
+    const int far = b->far_rule;
+    const spt::Layout L = spt::make_layout(spt::kFieldChunk, far);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+#define SPT_FIELD(F, R)                                                                                           \
+    {                                                                                                             \
+        rc = set_smem(spt::bem_field_kernel<F, R>, L.bytes);                                                       \
+        if (rc) return rc;                                                                                        \
+        spt::bem_field_kernel<F, R><<<(unsigned)blocks, spt::kMaxThreads, L.bytes, st>>>(x, y, z, n, *b, ex, ey, ez, \
+                                                                                       nullptr);                  \
+        return cuda_check(cudaGetLastError(), "bem_field_kernel launch");                                         \
+    }
+    if (form == SPT_FORM_FP64 && far == SPT_FAR_REFERENCE) SPT_FIELD(SPT_FORM_FP64, SPT_FAR_REFERENCE)
+    if (form == SPT_FORM_FP64) SPT_FIELD(SPT_FORM_FP64, SPT_FAR_ADAPTIVE)
+    if (far == SPT_FAR_REFERENCE) SPT_FIELD(SPT_FORM_MIXED, SPT_FAR_REFERENCE)
+    SPT_FIELD(SPT_FORM_MIXED, SPT_FAR_ADAPTIVE)
+#undef SPT_FIELD
 }
 
 int spt_surrogate_field(const double* x, const double* y, const double* z, int64_t n, const SptBem* b,
@@ -2357,13 +483,21 @@ int spt_surrogate_field(const double* x, const double* y, const double* z, int64
     if (rc) return rc;
     rc = check_surrogate_params(sur);
     if (rc) return rc;
-    const spt::Layout L = spt::make_layout(spt::kSurChunk, true, true);
-    rc = set_smem(spt::surrogate_field_kernel, L.bytes);
-    if (rc) return rc;
     const long long blocks = (n + spt::kSurChunk - 1) / spt::kSurChunk;
     if (blocks > 0x7fffffffLL) return fail(SPT_ERR_CAPACITY, "too many points");
-    spt::surrogate_field_kernel<<<(unsigned)blocks, spt::kThreads, L.bytes, static_cast<cudaStream_t>(stream)>>>(
-        x, y, z, n, *b, *sur, ex, ey, ez, nullptr);
+    const spt::Layout L = spt::make_layout(spt::kSurChunk, b->far_rule, true);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (b->far_rule == SPT_FAR_REFERENCE) {
+        rc = set_smem(spt::surrogate_field_kernel<SPT_FAR_REFERENCE>, L.bytes);
+        if (rc) return rc;
+        spt::surrogate_field_kernel<SPT_FAR_REFERENCE><<<(unsigned)blocks, spt::kMaxThreads, L.bytes, st>>>(
+            x, y, z, n, *b, *sur, ex, ey, ez, nullptr);
+    } else {
+        rc = set_smem(spt::surrogate_field_kernel<SPT_FAR_ADAPTIVE>, L.bytes);
+        if (rc) return rc;
+        spt::surrogate_field_kernel<SPT_FAR_ADAPTIVE><<<(unsigned)blocks, spt::kMaxThreads, L.bytes, st>>>(
+            x, y, z, n, *b, *sur, ex, ey, ez, nullptr);
+    }
     return cuda_check(cudaGetLastError(), "surrogate_field_kernel launch");
 }
 
@@ -2417,60 +551,70 @@ int spt_bem_assemble(const double* profile_rho, const double* profile_z, int32_t
 // library image: every GPU that loads the library holds its 4 MiB until the
 // process exits.  Host code cannot use `g_noalloc_scratch` as an address --
 // on the host that name is only a stand-in -- so its device address is
-// looked up once per device with cudaGetSymbolAddress, with that device
-// current, on the first call made on that device.
+// looked up with cudaGetSymbolAddress, with the device current, on the first
+// call in each CUDA context, and cached under that context's unique id: a
+// context created after a device reset (or a caller's own driver-API
+// context) loads the module again, possibly at another address, and gets a
+// fresh lookup.
 namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(4) << 20;
 }
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 namespace {
-void* g_noalloc_ptr[64] = {nullptr};
+struct NoAllocCache {
+    std::mutex mu;
+    unsigned long long ctx_id = 0;
+    void* ptr = nullptr;
+};
+NoAllocCache g_noalloc_cache[64];
+
+// Driver entry points for the context checks, looked up through the runtime
+// (the library does not link the driver library directly, so it loads on
+// machines without a GPU driver).
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+int driver_fn(const char* name, void** fn) {
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    const cudaError_t e = cudaGetDriverEntryPoint(name, fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !*fn)
+        return fail(SPT_ERR_CUDA, "driver entry point %s unavailable", name);
+    return SPT_OK;
+}
 
 int noalloc_scratch(void** out) {
     int dev = 0;
     int rc = cuda_check(cudaGetDevice(&dev), "cudaGetDevice");
     if (rc) return rc;
     if (dev < 0 || dev >= 64) return fail(SPT_ERR_CAPACITY, "device index %d above 63", dev);
-    if (!g_noalloc_ptr[dev]) {
+    void* f_cur = nullptr;
+    void* f_id = nullptr;
+    if ((rc = driver_fn("cuCtxGetCurrent", &f_cur)) || (rc = driver_fn("cuCtxGetId", &f_id))) return rc;
+    CUcontext ctx = nullptr;
+    if (reinterpret_cast<CtxGetCurrentFn>(f_cur)(&ctx) != CUDA_SUCCESS) return fail(SPT_ERR_CUDA, "cuCtxGetCurrent failed");
+    if (!ctx) {
+        // no context current yet: bind the device's primary context (what the runtime would use)
+        rc = cuda_check(cudaSetDevice(dev), "cudaSetDevice");
+        if (rc) return rc;
+        if (reinterpret_cast<CtxGetCurrentFn>(f_cur)(&ctx) != CUDA_SUCCESS || !ctx)
+            return fail(SPT_ERR_CUDA, "no current CUDA context");
+    }
+    unsigned long long id = 0;
+    if (reinterpret_cast<CtxGetIdFn>(f_id)(ctx, &id) != CUDA_SUCCESS) return fail(SPT_ERR_CUDA, "cuCtxGetId failed");
+    NoAllocCache& c = g_noalloc_cache[dev];
+    std::lock_guard<std::mutex> lock(c.mu);
+    if (!c.ptr || c.ctx_id != id) {
         void* p = nullptr;
         rc = cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress(g_noalloc_scratch)");
         if (rc) return rc;
-        g_noalloc_ptr[dev] = p;
+        c.ptr = p;
+        c.ctx_id = id;
     }
-    *out = g_noalloc_ptr[dev];
+    *out = c.ptr;
     return SPT_OK;
 }
 
-template <int KIND>
-int launch_trace_noalloc(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b,
-                         unsigned char* scratch, cudaStream_t stream) {
-    const spt::Layout L = spt::make_layout(s->max_group_size, true, p->form == SPT_FORM_SURROGATE);
-    auto kern = spt::trace_kernel<KIND>;
-    int rc = set_smem(kern, L.bytes);
-    if (rc) return rc;
-    int per_sm = 0;
-    rc = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, spt::kThreads, L.bytes), "occupancy");
-    if (rc) return rc;
-    if (per_sm < 1) return fail(SPT_ERR_CAPACITY, "group size %d does not fit one CTA", s->max_group_size);
-    int grid = grid_for(s->n_groups, per_sm);
-    double* slots = nullptr;
-    if (L.big) {
-        // the persistent grid is capped by the number of slope slots the fixed scratch holds
-        const size_t slot_bytes = spt::big_slot_doubles(s->max_group_size) * 8;
-        const long long fit = (long long)((kNoAllocScratchBytes - 256) / slot_bytes);
-        if (fit < 1) return fail(SPT_ERR_CAPACITY, "spt_trace_noalloc: one group buffer exceeds the %zu-byte scratch",
-                                 kNoAllocScratchBytes);
-        if (grid > fit) grid = (int)fit;
-        slots = reinterpret_cast<double*>(scratch + 256);
-    }
-    // the counter must start at zero; the slot buffers are written before they are read
-    rc = cuda_check(cudaMemsetAsync(scratch, 0, sizeof(int), stream), "cudaMemsetAsync");
-    if (rc) return rc;
-    SptBem bem = b ? *b : SptBem{};
-    kern<<<grid, spt::kThreads, L.bytes, stream>>>(*s, *p, *g, bem, reinterpret_cast<int*>(scratch), slots);
-    return cuda_check(cudaGetLastError(), "trace_kernel launch");
-}
 }  // namespace
 
 extern "C" int spt_trace_noalloc(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b,
@@ -2480,8 +624,8 @@ extern "C" int spt_trace_noalloc(const SptState* s, const SptTraceParams* p, con
     if (s->max_group_size <= 0 || s->max_group_size > 1024)
         return fail(SPT_ERR_CAPACITY, "spt_trace_noalloc: max_group_size %d outside [1, 1024]", s->max_group_size);
     if (s->n_active && !s->group_order) return fail(SPT_ERR_ARG, "n_active needs group_order");
-    if (p->form != SPT_FORM_FP64 && p->form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "unknown form %d", p->form);
     if (p->form == SPT_FORM_SURROGATE) return fail(SPT_ERR_ARG, "spt_trace_noalloc: the learned form is not offered");
+    if (p->form != SPT_FORM_FP64 && p->form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "unknown form %d", p->form);
     if (is_bem(g->kind)) {
         const int rc = check_bem(b);
         if (rc) return rc;
@@ -2489,14 +633,6 @@ extern "C" int spt_trace_noalloc(const SptState* s, const SptTraceParams* p, con
     void* scratch = nullptr;
     int rc = noalloc_scratch(&scratch);
     if (rc) return rc;
-    unsigned char* sc = static_cast<unsigned char*>(scratch);
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
-    switch (g->kind) {
-        case SPT_GEOM_FLAT: return launch_trace_noalloc<SPT_GEOM_FLAT>(s, p, g, b, sc, st);
-        case SPT_GEOM_TIP: return launch_trace_noalloc<SPT_GEOM_TIP>(s, p, g, b, sc, st);
-        case SPT_GEOM_TIP_BEM: return launch_trace_noalloc<SPT_GEOM_TIP_BEM>(s, p, g, b, sc, st);
-        case SPT_GEOM_WELL_BEM: return launch_trace_noalloc<SPT_GEOM_WELL_BEM>(s, p, g, b, sc, st);
-        case SPT_GEOM_POST_BEM: return launch_trace_noalloc<SPT_GEOM_POST_BEM>(s, p, g, b, sc, st);
-        default: return fail(SPT_ERR_ARG, "unknown geometry kind %d", g->kind);
-    }
+    return run_trace(s, p, g, b, static_cast<unsigned char*>(scratch), (int64_t)kNoAllocScratchBytes,
+                     static_cast<cudaStream_t>(stream), "spt_trace_noalloc");
 }

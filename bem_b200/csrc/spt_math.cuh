@@ -26,17 +26,17 @@ constexpr double kPi = 3.141592653589793;
 // b_n, b_n (d_n - 1/((2n+1)(2n+2)))), n = 0..9, computed from the
 // recurrences a_n = a_{n-1}(n-1/2)/n, b_n = b_{n-1}(n-1/2)(n+1/2)/((n+1)n),
 // d_n = d_{n-1} - 1/(n(2n-1)), d_0 = 2 ln 2.
-__device__ __constant__ double kSerK[10] = {
+static __device__ __constant__ double kSerK[10] = {
     1.0, 0.25, 0.140625, 0.09765625, 0.07476806640625, 0.0605621337890625,
     0.050889015197753906, 0.043878793716430664, 0.03856534603983164, 0.034399336436763406};
-__device__ __constant__ double kSerKd[10] = {
+static __device__ __constant__ double kSerKd[10] = {
     1.3862943611198906, 0.09657359027997264, 0.030885144532484612, 0.01493760036978098,
     0.008766312197176064, 0.0057548876844001106, 0.004064658549993974, 0.003022546550344074,
     0.0023351571703480825, 0.0018580702734561816};
-__device__ __constant__ double kSerE[10] = {
+static __device__ __constant__ double kSerE[10] = {
     1.0, 0.375, 0.234375, 0.1708984375, 0.13458251953125, 0.11103057861328125,
     0.09450817108154297, 0.0822727382183075, 0.0728456536307931, 0.06535873922985047};
-__device__ __constant__ double kSerEd[10] = {
+static __device__ __constant__ double kSerEd[10] = {
     0.8862943611198906, 0.11361038541995896, 0.043662740887474356, 0.023089042834616717,
     0.014284000626791913, 0.00970948667432989, 0.007029375927562748, 0.005324471705985524,
     0.004172794741275812, 0.0033583368373829277};
@@ -147,33 +147,44 @@ __device__ __forceinline__ void ring_field_far(double rho, double inv_rho, doubl
 }
 
 // ---------------------------------------------------------------------------
-// float32 variants (SPT_FORM_MIXED).  Same methods; the series branch is
-// used below p < 1e-2 with four terms (truncation < 1e-9), the AGM above.
+// float32 variants (SPT_FORM_MIXED).
+//
+// K(1-p), E(1-p) for p >= 1e-3 from the polynomial-logarithmic
+// approximations of C. Hastings Jr. (Approximations for Digital Computers,
+// 1955) as tabulated in Abramowitz & Stegun, Handbook of Mathematical
+// Functions, 17.3.34 (K) and 17.3.36 (E), with m1 = 1 - m = p:
+//   K = sum_{i<=4} a_i p^i + ln(1/p) sum_{i<=4} b_i p^i,   |error| <= 2e-8,
+//   E = 1 + sum_{1<=i<=4} c_i p^i + ln(1/p) sum_{1<=i<=4} d_i p^i,  |error| <= 2e-8
+// (checked against SciPy's ellipkm1/ellipe: 1.3e-8 and 1.6e-8 at most on
+// p in [1e-6, 1]), below float32 rounding: one logarithm and four degree-4
+// Horner chains instead of the AGM's six square roots.
+__device__ __forceinline__ void ellip_ke_hastings_f(float p, float& K, float& E) {
+    const float L = -__logf(p);
+    const float ka = fmaf(fmaf(fmaf(fmaf(0.01451196212f, p, 0.03742563713f), p, 0.03590092383f), p, 0.09666344259f), p,
+                          1.38629436112f);
+    const float kb = fmaf(fmaf(fmaf(fmaf(0.00441787012f, p, 0.03328355346f), p, 0.06880248576f), p, 0.12498593597f), p,
+                          0.5f);
+    const float ea = fmaf(fmaf(fmaf(fmaf(0.01736506451f, p, 0.04757383546f), p, 0.06260601220f), p, 0.44325141463f), p,
+                          1.0f);
+    const float eb = fmaf(fmaf(fmaf(0.00526449639f, p, 0.04069697526f), p, 0.09200180037f), p, 0.24998368310f) * p;
+    K = fmaf(kb, L, ka);
+    E = fmaf(eb, L, ea);
+}
+
+// The series branch (DLMF 19.12, four terms, truncation < 1e-9) below
+// p = 1e-2, Hastings above.
 __device__ __forceinline__ void ellip_ke_f(float p, float& K, float& E) {
-    if (p < 1e-2f) {
-        const float L = -0.5f * __logf(p);
-        const float A = fmaf(fmaf(fmaf(0.09765625f, p, 0.140625f), p, 0.25f), p, 1.0f);
-        const float B = fmaf(fmaf(fmaf(0.01493760037f, p, 0.03088514453f), p, 0.09657359028f), p, 1.386294361f);
-        const float C = fmaf(fmaf(fmaf(0.1708984375f, p, 0.234375f), p, 0.375f), p, 1.0f);
-        const float D = fmaf(fmaf(fmaf(0.02308904283f, p, 0.04366274089f), p, 0.1136103854f), p, 0.8862943611f);
-        K = fmaf(L, A, B);
-        E = fmaf(0.5f * p, fmaf(L, C, D), 1.0f);
+    if (p >= 1e-2f) {
+        ellip_ke_hastings_f(p, K, E);
         return;
     }
-    float a = 1.0f, b = sqrtf(p);
-    float S = 0.5f * (1.0f - p), w = 0.5f;
-#pragma unroll 1
-    for (int it = 0; it < 8; ++it) {
-        const float c = 0.5f * (a - b);
-        const float an = 0.5f * (a + b);
-        b = sqrtf(a * b);
-        a = an;
-        w += w;
-        S = fmaf(w * c, c, S);
-        if (fabsf(c) <= 3e-8f * a) break;
-    }
-    K = 1.5707963267948966f / a;
-    E = K * (1.0f - S);
+    const float L = -0.5f * __logf(p);
+    const float A = fmaf(fmaf(fmaf(0.09765625f, p, 0.140625f), p, 0.25f), p, 1.0f);
+    const float B = fmaf(fmaf(fmaf(0.01493760037f, p, 0.03088514453f), p, 0.09657359028f), p, 1.386294361f);
+    const float C = fmaf(fmaf(fmaf(0.1708984375f, p, 0.234375f), p, 0.375f), p, 1.0f);
+    const float D = fmaf(fmaf(fmaf(0.02308904283f, p, 0.04366274089f), p, 0.1136103854f), p, 0.8862943611f);
+    K = fmaf(L, A, B);
+    E = fmaf(0.5f * p, fmaf(L, C, D), 1.0f);
 }
 
 __device__ __forceinline__ void ring_field_f(float rho, float z, float a, float& er, float& ez) {
@@ -197,37 +208,6 @@ __device__ __forceinline__ void ring_field_f(float rho, float z, float a, float&
     ez = z * E * rsD * inv_d2 * (1.0f / (2.0f * 9.8696044f));
 }
 
-
-// float32 K, E for the far sum of the mixed form: the 4-term DLMF 19.12
-// series below p = 1e-2, a fixed five-step AGM above (for p >= 1e-2 the fifth
-// half-difference is below 1e-9, so a_5 has converged to float precision).
-// Callers send p < 1e-3 to the float64 path instead.
-__device__ __forceinline__ void ellip_ke_f_fixed(float p, float& K, float& E) {
-    if (p < 1e-2f) {
-        const float L = -0.5f * __logf(p);
-        const float A = fmaf(fmaf(fmaf(0.09765625f, p, 0.140625f), p, 0.25f), p, 1.0f);
-        const float B = fmaf(fmaf(fmaf(0.01493760037f, p, 0.03088514453f), p, 0.09657359028f), p, 1.386294361f);
-        const float C = fmaf(fmaf(fmaf(0.1708984375f, p, 0.234375f), p, 0.375f), p, 1.0f);
-        const float D = fmaf(fmaf(fmaf(0.02308904283f, p, 0.04366274089f), p, 0.1136103854f), p, 0.8862943611f);
-        K = fmaf(L, A, B);
-        E = fmaf(0.5f * p, fmaf(L, C, D), 1.0f);
-        return;
-    }
-    float a = 1.0f, b = p * rsqrtf(p);
-    float S = 0.5f * (1.0f - p), w = 0.5f;
-#pragma unroll
-    for (int it = 0; it < 5; ++it) {
-        const float c = 0.5f * (a - b);
-        const float an = 0.5f * (a + b);
-        const float ab = a * b;
-        b = ab * rsqrtf(ab);
-        a = an;
-        w += w;
-        S = fmaf(w * c, c, S);
-    }
-    K = 1.5707963267948966f * __frcp_rn(a);
-    E = K * (1.0f - S);
-}
 
 // float32 unit-ring field near the axis: with r^2 = a^2 + z^2, x = rho / r and
 // t = z / r, the potential of the ring expands in Legendre polynomials of t
@@ -271,8 +251,8 @@ __device__ __forceinline__ void ring_axis_f(float rho, float z, float a, float& 
 // float32 ring field for the far sum of the mixed form.  dr = rho - a and
 // sr = rho + a are formed in float64 by the caller (rho and a are close near
 // a wall), then rounded.  Near the axis (rho^2 < 0.09 (a^2 + z^2)) the
-// Legendre expansion above; elsewhere K and E from a fixed six-step float AGM
-// (converged for p >= 1e-3) -- the radial formula's cancellation there costs
+// Legendre expansion above; elsewhere K and E from the Hastings
+// approximations (p >= 1e-3) -- the radial formula's cancellation there costs
 // at most ~eps_f / x of the ring's field scale.  Returns false (the caller
 // evaluates the pair in float64) when p = d2 / D < 1e-3: the point is close
 // to the ring itself.
@@ -288,21 +268,8 @@ __device__ __forceinline__ bool ring_far_f(float rho, float inv_rho, float dr, f
     const float invD = __frcp_rn(D);
     const float p = d2 * invD;
     const bool ok = p >= 1e-3f;
-    const float pc = fmaxf(p, 1e-3f);
-    float aa = 1.0f, bb = pc * rsqrtf(pc);
-    float S = 0.5f * (1.0f - pc), w = 0.5f;
-#pragma unroll
-    for (int it = 0; it < 6; ++it) {
-        const float c = 0.5f * (aa - bb);
-        const float an = 0.5f * (aa + bb);
-        const float ab = aa * bb;
-        bb = ab * rsqrtf(ab);
-        aa = an;
-        w += w;
-        S = fmaf(w * c, c, S);
-    }
-    const float K = 1.5707963267948966f * __frcp_rn(aa);
-    const float E = K * (1.0f - S);
+    float K, E;
+    ellip_ke_hastings_f(fminf(fmaxf(p, 1e-3f), 1.0f), K, E);
     const float inv_d2 = __frcp_rn(d2);
     const float rsD = rsqrtf(D);
     er = (K - (a2 - rho2 + z2) * E * inv_d2) * (rsD * inv_rho * 0.025330295910584444f);  // 1/(4 pi^2)

@@ -22,7 +22,7 @@ import numpy as np
 def points_for_length(arc, max_length, min_points=2):
     """Node count so that each of the (n-1) segments is at most max_length."""
     if max_length <= 0.0:
-        raise ValueError(f"max_length must be positive (got {max_length!r})")
+        raise ValueError(f"segment length bound {max_length!r} is not > 0")
     return max(min_points, max(1, int(np.ceil(arc / max_length))) + 1)
 
 

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define SPT_ABI_VERSION 1
+#define SPT_ABI_VERSION 2
 
 /* return codes */
 #define SPT_OK 0
@@ -75,7 +75,9 @@ extern "C" {
 #define SPT_CNT_NEAR_PAIRS 7         /* (point, segment) pairs handled by the near quadrature */
 #define SPT_CNT_FP64_ROUNDS 8        /* mixed form: far-sum rounds recomputed in float64 (ill-conditioned) */
 #define SPT_CNT_FP64_TARGETS 9       /* mixed form: pair-sum targets recomputed in float64 */
-#define SPT_N_COUNTERS 10
+#define SPT_CNT_LIVE_STEPS 10        /* sum over accepted group-steps of the particles alive (born, not
+                                        killed) at the step start */
+#define SPT_N_COUNTERS 11
 
 /* Geometry parameters.  Fields a kind does not use are ignored. */
 typedef struct {
@@ -239,7 +241,13 @@ typedef struct {
      * round's classification.  Results agree to rounding (and, with the
      * adaptive rule, to its ~1e-14 classification effect). */
     int32_t round_points;
-    int32_t reserved2;
+    /* CTA width of the trace: 32, 64, 128 or 256 threads work on one group
+     * at a time (0 or anything else: by group size -- 64 up to 16
+     * particles, 128 up to 64, else 256; 256 with the reference far rule;
+     * at least 128 for the learned form).  Narrower CTAs put more groups on
+     * an SM and fewer warps behind each barrier.  Results do not depend on
+     * it beyond the summation order of the reductions. */
+    int32_t cta_threads;
     /* Mixed form: a float32 far-sum round or pair sum whose sum of |terms|
      * exceeds kappa_max times the whole field (uniform included) or the
      * whole acceleration at a point is recomputed in float64 -- the float32
@@ -247,6 +255,11 @@ typedef struct {
      * regions, where the perturbation cancels the uniform field; dense
      * bunches).  0: the default, 16. */
     double kappa_max;
+    /* Largest persistent grid (CTAs) of this launch; 0: the whole GPU (SMs x
+     * resident CTAs).  Launches of different group-size bins on concurrent
+     * streams share the SMs by giving each a grid in proportion to its work. */
+    int32_t max_ctas;
+    int32_t reserved3;
 } SptTraceParams;
 
 /* Scratch bytes spt_trace needs for this state/geometry (work-queue
@@ -334,9 +347,11 @@ int spt_bem_assemble(const double* profile_rho, const double* profile_z, int32_t
  *     groups above 256 particles the scratch holds floor((4 MiB - 256) /
  *     (432 * max_group_size)) per-CTA buffers, which caps the number of
  *     CTAs that run at once (9 at 1024 particles).
- *   - The first call on a device looks the array's address up
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture.
+ *   - The first call in each CUDA context (the current device's primary
+ *     context, or the caller's own driver-API context) looks the array's
+ *     address up (cudaGetSymbolAddress) with that device current and caches
+ *     it under the context's id; make that first call before any stream
+ *     capture.  After a device reset the next call looks it up again.
  *   - Every call shares the one array: calls that overlap on the GPU (other
  *     streams, other host threads) race on it; serialise them.  Each call
  *     clears the work-queue counter it needs; nothing else carries over. */
