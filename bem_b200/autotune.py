@@ -2,8 +2,12 @@
 
 The knobs change speed, not physics:
 
+* ``cta_threads`` -- the CTA width (64, 128, 256 threads on one group at a
+  time): narrower CTAs put more groups on an SM and fewer warps behind each
+  barrier; wider ones spread a large group's work.  Results agree to the
+  summation order of the reductions.
 * ``round_points`` -- the far-sum tile shape: evaluation points per round
-  (1, 2, 4, 8).  Fewer points give each thread more nodes in flight per
+  (1, 2, 4).  Fewer points give each thread more nodes in flight per
   point; more points share node loads and the adaptive rule's
   classification.  Results agree to rounding.
 * ``ratios`` -- thresholds (ratio4, ratio2, ratio_run) of the adaptive far
@@ -18,11 +22,12 @@ largest first (a sample once preferred the given order, which then cost the
 full C1 launch 8 %).
 
 Procedure: a sample of groups (every k-th group, so that every size range is
-represented) is advanced `warm` attempts from emission, the warmed state is
-saved, and each candidate runs `attempts` attempts from that state, timed
-with CUDA events (best of `repeats`).  Coordinate descent: round_points,
-then ratios; a candidate replaces the current choice only if it is faster by
-more than `margin` (timing noise on a sample is a few per cent).  The winner
+represented; 2368 = 16 per SM, enough to fill the GPU at every CTA width) is
+advanced `warm` attempts from emission, the warmed state is saved, and each
+candidate runs `attempts` attempts from that state, timed with CUDA events
+(best of `repeats`).  Coordinate descent: cta_threads, round_points, then
+ratios; a candidate replaces the current choice only if it is faster by more
+than `margin` (timing noise on a sample is a few per cent).  The winner
 is applied to a Tracer / GroupBatch with ``apply``.  Results can be cached
 in a JSON file keyed by the geometry, form, rule and group-size mix.
 """
@@ -34,7 +39,8 @@ import numpy as np
 
 from . import _lib, engine, tables
 
-ROUND_POINTS = (8, 4, 2)
+CTA_THREADS = (64, 128, 256)
+ROUND_POINTS = (4, 2, 1)
 RATIOS = ((tables.RATIO4, tables.RATIO2, tables.RATIO_RUN), (6.0, 150.0, 3.0), (12.0, 600.0, 6.0),
           (16.0, 1000.0, 8.0))
 ORDERS = ("largest_first",)
@@ -55,7 +61,7 @@ def signature(tracer, sizes):
 
 
 class TuneResult(dict):
-    """config (round_points, ratios, order) plus the timings behind it."""
+    """config (cta_threads, round_points, ratios, order) plus the timings behind it."""
 
 
 def _sample(sizes, n_sample):
@@ -82,8 +88,8 @@ def _accuracy_ok(tracer, pos, ratios, tol):
 
 
 def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plummer_radius, charge_to_mass,
-         n_sample=592, warm=48, attempts=16, repeats=3, tol=1e-11, margin=0.03, cache=None):
-    """Choose round_points and the adaptive rule's ratios for `tracer` on
+         n_sample=2368, warm=200, attempts=32, repeats=3, tol=1e-11, margin=0.03, cache=None, threads=CTA_THREADS):
+    """Choose the CTA width, round_points and the adaptive rule's ratios for `tracer` on
     this workload (arrays as for GroupBatch; the order stays largest first).  Returns a
     TuneResult; `apply` sets it.  `cache`: a JSON file path (read if it holds
     this signature, updated otherwise)."""
@@ -101,13 +107,14 @@ def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plum
     sub = (np.asarray(pos)[rows], np.asarray(vel)[rows], np.asarray(t_birth)[rows], np.asarray(charge)[rows],
            np.asarray(mass)[rows], sizes[groups])
     base = engine.GroupBatch(*sub, device=tracer.device)
-    prm = lambda a, rp=None: tracer.params(t_max, rtol, atol, plummer_radius, charge_to_mass, a, round_points=rp)
+    prm = lambda a, rp=None, th=None: tracer.params(t_max, rtol, atol, plummer_radius, charge_to_mass, a,
+                                                    round_points=rp, cta_threads=th)
     tracer.launch(base, prm(warm))
     torch.cuda.synchronize()
     work = engine.GroupBatch(*sub, device=tracer.device)
-    saved_bem, saved_rp = tracer.bem, tracer.round_points
+    saved_bem, saved_rp, saved_th = tracer.bem, tracer.round_points, tracer.cta_threads
 
-    def timed(order, rp, ratios):
+    def timed(order, rp, ratios, th=0):
         if tracer.tables is not None:
             tracer.bem = tracer.tables.view(tracer.far_rule, ratio4=ratios[0], ratio2=ratios[1], ratio_run=ratios[2])
         work.set_order(order)
@@ -118,7 +125,7 @@ def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plum
             c0 = tracer.counter_dict()["particle_steps"]
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record()
-            tracer.launch(work, prm(attempts, rp))
+            tracer.launch(work, prm(attempts, rp, th))
             e.record()
             e.synchronize()
             best = min(best, s.elapsed_time(e) * 1e-3)
@@ -126,17 +133,22 @@ def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plum
         return steps / best
 
     timings = {}
-    cfg = dict(round_points=8, ratios=list(RATIOS[0]), order="largest_first")
+    cfg = dict(cta_threads=0, round_points=4, ratios=list(RATIOS[0]), order="largest_first")
 
     def pick(rates, current):
         best = max(rates, key=rates.get)
         return best if rates[best] > (1.0 + margin) * rates[current] else current
 
     try:
+        if len(threads) > 1 or threads[0]:
+            rates = {}
+            for th in threads:
+                rates[th] = timings[f"cta_threads={th}"] = timed(cfg["order"], cfg["round_points"], cfg["ratios"], th)
+            cfg["cta_threads"] = max(rates, key=rates.get)
         rates = {}
         for rp in ROUND_POINTS:
-            rates[rp] = timings[f"round_points={rp}"] = timed(cfg["order"], rp, cfg["ratios"])
-        cfg["round_points"] = pick(rates, 8)
+            rates[rp] = timings[f"round_points={rp}"] = timed(cfg["order"], rp, cfg["ratios"], cfg["cta_threads"])
+        cfg["round_points"] = pick(rates, 4)
         if tracer.tables is not None and tracer.far_rule == "adaptive":
             sample_pos = base.positions().cpu().numpy()
             rates = {}
@@ -144,13 +156,13 @@ def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plum
                 if not _accuracy_ok(tracer, sample_pos, r, tol):
                     timings[f"ratios={r}"] = "rejected by the accuracy guard"
                     continue
-                rates[r] = timings[f"ratios={r}"] = timed(cfg["order"], cfg["round_points"], r)
+                rates[r] = timings[f"ratios={r}"] = timed(cfg["order"], cfg["round_points"], r, cfg["cta_threads"])
             if RATIOS[0] in rates:
                 cfg["ratios"] = list(pick(rates, RATIOS[0]))
             elif rates:
                 cfg["ratios"] = list(max(rates, key=rates.get))
     finally:
-        tracer.bem, tracer.round_points = saved_bem, saved_rp
+        tracer.bem, tracer.round_points, tracer.cta_threads = saved_bem, saved_rp, saved_th
     res = TuneResult(cfg, timings=timings, key=key, sample_groups=len(groups), attempts=attempts, warm=warm)
     if cache:
         stored = {}
@@ -166,6 +178,7 @@ def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plum
 def apply(config, tracer, batch=None):
     """Set a tuned configuration on a Tracer (and a GroupBatch's order)."""
     tracer.round_points = int(config["round_points"])
+    tracer.cta_threads = int(config.get("cta_threads", 0))
     if tracer.tables is not None:
         r = config["ratios"]
         tracer.bem = tracer.tables.view(tracer.far_rule, ratio4=r[0], ratio2=r[1], ratio_run=r[2])

@@ -17,6 +17,7 @@ from . import _lib
 from .constants import COULOMB_CONSTANT
 
 DEFAULT_ATTEMPT_CHUNK = 4096  # attempts per group per launch; the host loops until every group is done
+DEFAULT_BINS = ((8, 64), (64, 128), (1024, 256))  # (largest group size, CTA width) of size-binned launches
 
 
 def _torch():
@@ -120,6 +121,33 @@ class GroupBatch:
                                                  self.n_active.data_ptr(), ctypes.c_void_p(stream.cuda_stream)),
                    "spt_compact_groups")
 
+    def bin_plan(self, bins=None):
+        """Size-binned scheduling: the groups split by size into bins, each
+        traced by its own launch with its own CTA width (Tracer.launch_binned).
+        bins: ((largest group size, CTA width), ...) ascending; the default
+        puts groups of 1-8 particles on 64-thread CTAs, 9-64 on 128, larger
+        on 256.  Returns one entry per non-empty bin: the device order of its
+        groups (largest first), their count and largest size, the CTA width,
+        and the bin's share of the estimated work (partition.group_cost)."""
+        torch = _torch()
+        from .partition import group_cost
+        bins = DEFAULT_BINS if bins is None else bins
+        cost = group_cost(self.sizes)
+        total = float(cost.sum())
+        plan, lo = [], 0
+        for hi, threads in bins:
+            idx = np.nonzero((self.sizes > lo) & (self.sizes <= hi))[0]
+            lo = hi
+            if len(idx) == 0:
+                continue
+            idx = idx[np.argsort(-self.sizes[idx], kind="stable")].astype(np.int32)
+            plan.append(dict(order=torch.as_tensor(idx, device=self.device), n=len(idx),
+                             max_size=int(self.sizes[idx].max()), threads=int(threads),
+                             share=float(cost[idx].sum()) / total))
+        if sum(b["n"] for b in plan) != self.n_groups:
+            raise ValueError("the bins do not cover every group size")
+        return plan
+
     def struct(self):
         s = _lib.SptState()
         s.n_groups = self.n_groups
@@ -171,7 +199,8 @@ class Tracer:
         self.geom = geometry.to_struct(z_max=z_max)
         self.tables = geometry.bem_tables(self.device) if geometry.is_bem else None
         self.far_rule = far_rule
-        self.round_points = 0  # far-sum points per round (0: the kernel's default, 8); see autotune
+        self.round_points = 0  # far-sum points per round (0: the kernel's default, 4); see autotune
+        self.cta_threads = 0   # CTA width, 32/64/128/256 (0: the library's choice by group size); see autotune
         self.kappa_max = 0.0   # mixed form's conditioning bound for float32 sums (0: the kernel's default, 16)
         self.bem = None
         if self.tables is not None:
@@ -187,9 +216,10 @@ class Tracer:
 
     def params(self, t_max, rtol, atol, plummer_radius, charge_to_mass, max_attempts, log=None,
                safety=0.9, min_factor=0.2, max_factor=10.0, initial_step_fraction=1e-6,
-               coulomb_constant=COULOMB_CONSTANT, records=None, round_points=None, kappa_max=None):
+               coulomb_constant=COULOMB_CONSTANT, records=None, round_points=None, kappa_max=None, cta_threads=None):
         p = _lib.SptTraceParams()
         p.round_points = int(self.round_points if round_points is None else round_points)
+        p.cta_threads = int(self.cta_threads if cta_threads is None else cta_threads)
         p.kappa_max = float(self.kappa_max if kappa_max is None else kappa_max)
         p.t_max, p.rtol, p.atol = float(t_max), float(rtol), float(atol)
         p.plummer_radius = float(plummer_radius)
@@ -237,11 +267,59 @@ class Tracer:
                                         ctypes.c_void_p(ws.data_ptr()), ws.numel(),
                                         ctypes.c_void_p(stream.cuda_stream)), "spt_trace")
 
+    def launch_binned(self, batch, params, plan, stream=None):
+        """One spt_trace launch per size bin of `plan` (GroupBatch.bin_plan),
+        each on its own stream with its own CTA width and a persistent grid
+        in proportion to its share of the work, so the bins run side by side
+        and fill each other's tails.  The launches share the batch's arrays
+        (disjoint groups) and are joined back into `stream`."""
+        torch = _torch()
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device)
+        if not hasattr(self, "_bin_streams"):
+            self._bin_streams, self._bin_ws = [], []
+        while len(self._bin_streams) < len(plan):
+            self._bin_streams.append(torch.cuda.Stream(self.device))
+            self._bin_ws.append(None)
+        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        ready = torch.cuda.Event()
+        ready.record(stream)
+        bem = ctypes.byref(self.bem) if self.bem is not None else None
+        for b, binfo in enumerate(plan):
+            st = batch.struct()
+            st.group_order = binfo["order"].data_ptr()
+            st.n_active = None
+            st.n_groups = binfo["n"]
+            st.max_group_size = binfo["max_size"]
+            p = _lib.SptTraceParams()
+            ctypes.pointer(p)[0] = params
+            p.cta_threads = binfo["threads"]
+            full = sms * max(1, 65536 // (128 * binfo["threads"]))  # resident CTAs at 128 registers a thread
+            p.max_ctas = max(1, int(np.ceil(full * binfo["share"])))
+            nbytes = ctypes.c_int64(0)
+            _lib.check(_lib.lib().spt_trace_workspace_bytes(ctypes.byref(st), ctypes.byref(p), ctypes.byref(self.geom),
+                                                            bem, ctypes.byref(nbytes)), "spt_trace_workspace_bytes")
+            need = max(int(nbytes.value), 256)
+            if self._bin_ws[b] is None or self._bin_ws[b].numel() < need:
+                self._bin_ws[b] = torch.empty(need, dtype=torch.uint8, device=self.device)
+            ws = self._bin_ws[b]
+            s = self._bin_streams[b]
+            s.wait_event(ready)
+            _lib.check(_lib.lib().spt_trace(ctypes.byref(st), ctypes.byref(p), ctypes.byref(self.geom), bem,
+                                            ctypes.c_void_p(ws.data_ptr()), ws.numel(), ctypes.c_void_p(s.cuda_stream)),
+                       "spt_trace")
+            done = torch.cuda.Event()
+            done.record(s)
+            stream.wait_event(done)
+
     def run(self, batch, t_max, rtol, atol, plummer_radius, charge_to_mass, max_steps=10_000_000,
             attempt_chunk=DEFAULT_ATTEMPT_CHUNK, log_capacity=0, screens=None, output_times=None,
-            screen_capacity=None, compact=False, graph=False, graph_launches=4, **kw):
+            screen_capacity=None, compact=False, graph=False, graph_launches=4, bins=None, **kw):
         """Integrate every group to t_max.  Raises RuntimeError when a group
         needs more than max_steps attempts (batched_rk45.py:320-321).
+
+        bins: size-binned scheduling -- a GroupBatch.bin_plan (or True for the
+        default bins): one launch per size bin on concurrent streams.
 
         With `screens` (z planes) and/or `output_times`, returns a
         TraceRecords holding every crossing and every output-time snapshot;
@@ -258,6 +336,11 @@ class Tracer:
                 raise ValueError("graph=True records neither screens, output times nor attempt logs")
             return self._run_graph(batch, t_max, rtol, atol, plummer_radius, charge_to_mass, max_steps,
                                    attempt_chunk, graph_launches, **kw)
+        plan = None
+        if bins is not None and bins is not False:
+            if compact:
+                raise ValueError("size-binned launches take their own group orders; compact=False")
+            plan = batch.bin_plan() if bins is True else bins
         if compact:
             batch.enable_compaction()
         records = None
@@ -276,7 +359,10 @@ class Tracer:
             p = self.params(t_max, rtol, atol, plummer_radius, charge_to_mass, chunk, log=log, **kw)
             if compact:
                 batch.compact()
-            self.launch(batch, p)
+            if plan is not None:
+                self.launch_binned(batch, p, plan)
+            else:
+                self.launch(batch, p)
             done_attempts += chunk
             if records is not None:
                 records.collect()

@@ -2,17 +2,15 @@
 tracer's hot path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload c1|c0|c2|c3|c4] [--attempts A] [--form fp64|mixed]
-                    [--far-rule reference|adaptive] [--no-tune]
+                    [--workload c1|c0|c2|c3|c4] [--span trace|slice] [--t-end T]
+                    [--form mixed|fp64] [--far-rule adaptive|reference]
+                    [--cta-threads 64|128|256] [--bins] [--no-tune] ...
 
 The chosen form (the default): float32 + Kahan BEM and pair sums (float64
 state, stage combination, error norm and controller, float64 for points
 close to a ring and for ill-conditioned sums) with the adaptive far-field
 rule, its launch configuration chosen first by the project's autotuner on a
-sample of the workload (untimed; `--no-tune` keeps the defaults).  The plain form (float64,
-the reference's quadrature) is timed in the same run on the same workload
-(`plain_fp64`), and `accuracy` reports the chosen form's endpoint error
-against it on a sample of groups traced to a fixed time.
+sample of the workload (untimed; `--no-tune` keeps the defaults).
 
 Workload (default c1, the largest single-GPU configuration with a BEM
 field): hemisphere R = 50 nm on a 5 um post, E = -1e6 V/m, 2000-panel BEM
@@ -20,17 +18,36 @@ capsule (64,000 far nodes), 4096 groups x 32 electrons, Coulomb + 3-image
 forces, rtol 1e-9, atol 1e-12, z_max = 1 mm, seed 1.  Synthetic, seeded
 inputs (workloads.py) stand in for a distgen distribution.
 
-A step is one spt_trace call that advances every group by at most A
-Dormand-Prince attempts, continuing from the state the previous step left
-(the trace is cut into slices, the way a long run is checkpointed).  W warm-up
-steps are followed by K timed steps; L2 is flushed (256 MiB write) between
-steps and each step is timed alone with CUDA events on the launch stream.
-value = accepted particle-steps (device counter: sum over accepted
-group-steps of the group size) / summed step time.
+A step (--span trace, the default) is one WHOLE trace of the workload: every
+group from its emission to t_end (C1: 20 ps, 19 ps past the last birth; the
+integrator's t_max is t_end), in one persistent spt_trace launch (one per
+size bin with --bins), from the same initial state each step (restored
+untimed).  W warm-up steps, then K timed steps; L2 is flushed (256 MiB
+write) before each step and each step is timed alone with CUDA events on the
+launch stream.  value = accepted particle-steps (device counter: sum over
+accepted group-steps of the group size) / summed step time.
+`live_particle_steps_per_s` counts only the particles alive at each
+accepted step.  --span slice times --attempts attempts per group per step
+instead, continuing from the previous step (labelled in config).
 
-N > 1 (torchrun): weak scaling -- every rank traces its own 4096 groups
-(seed + rank); there is no data-path collective, only a barrier and a max
-of the per-rank times.
+In the same run (rank 0):
+  plain_fp64  the plain form (float64, the reference's quadrature) traces the
+              first --plain-groups groups over the same span; the chosen form
+              traces the same groups; ratio = chosen / plain on that subset.
+  accuracy    endpoint error of the chosen form against the plain form on
+              that subset (alive particles by position and velocity, killed
+              ones by death time), and their attempt counts.
+  e2e         the same whole traces through the public API with the state in
+              pinned host memory: H2D of the initial state, the trace, D2H of
+              the final state, every step.
+  cpu_baseline  the oracle port (the reference's algorithm) on the host
+              cores, on a bounded prefix of the same trace.
+
+N > 1 (torchrun): the workload is N x the groups (one draw of N x 4096
+groups for C1), split into contiguous group ranges balanced by estimated
+cost (partition.py; weak scaling); each rank traces its range; the final
+state is all-gathered (NCCL) inside each timed step; times are the max over
+ranks.
 """
 
 import argparse
@@ -50,56 +67,63 @@ METRIC = "accepted RK45 particle-steps/s at ≤1e-6 rel endpoint err: chosen for
 UNIT = "particle-steps/s"
 FLOP_PER_RING = 64.0   # nominal FLOPs of one ring-kernel evaluation (26 algebra + 38 for K, E)
 FLOP_PER_PAIR = 20.0   # nominal FLOPs of one softened pair interaction
+WHOLE_TRACE = 1_000_000  # attempt budget of a whole-trace launch (every group reaches t_end far sooner)
+T_END = dict(c0=None, c1=20e-12, c2=20e-12, c3=30e-12, c4=20e-12)
 
 
 # ---------------------------------------------------------------------------
 # workloads
 
-def build_workload(name, rank=0):
-    """Returns dict(geometry, data, rtol, atol, t_max, z_max, label, config)."""
+def build_workload(name, n_copies=1):
+    """Returns dict(geometry, data, rtol, atol, t_max, z_max, config).
+    n_copies > 1: the same sampler drawn at n_copies x the groups (the
+    multi-GPU workload, partitioned across ranks)."""
     from bem_b200 import geometry as bg
     from bem_b200 import workloads as w
 
     if name == "c0":
         geo = bg.FlatCathode(-1e7, z0=3e-9, kill_z_below=0.0)
-        data = w.flat_c0(seed=0 + rank)
+        data = w.flat_c0(n_groups=16 * n_copies, seed=0)
         return dict(geometry=geo, data=data, rtol=1e-8, atol=1e-12, t_max=w.default_t_max(-1e7, 1e-3, 1e-12),
-                    z_max=1e-3, config=dict(workload="C0 flat cathode, 16 groups x 64, rtol 1e-8", groups=16,
-                                            group_size=64, bem_panels=0))
+                    z_max=1e-3, config=dict(workload=f"C0 flat cathode, {16 * n_copies} groups x 64, rtol 1e-8",
+                                            groups=16 * n_copies, group_size=64, bem_panels=0))
     if name in ("c1", "c2", "c4"):
         geo = bg.PostTipBEMGeometry(-1e6, 50e-9, 5e-6, n_cap=100, n_wall=900, n_subdiv=8, z0=3e-9)
         if name == "c1":
-            data = w.tip_c1(geo.profile, geo.sigma, seed=1 + rank)
-            cfg = dict(workload="C1 hemisphere-on-post BEM tip, 4096 groups x 32, 2000 panels, rtol 1e-9",
-                       groups=4096, group_size=32)
+            G = 4096 * n_copies
+            data = w.tip_c1(geo.profile, geo.sigma, n_groups=G, seed=1)
+            cfg = dict(workload=f"C1 hemisphere-on-post BEM tip, {G} groups x 32, 2000 panels, rtol 1e-9",
+                       groups=G, group_size=32)
         elif name == "c2":
-            data = w.tip_c2(seed=2 + rank)
-            cfg = dict(workload="C2 post tip, 512 groups x 1024, 2000 panels", groups=512, group_size=1024)
+            G = 512 * n_copies
+            data = w.tip_c2(n_groups=G, seed=2)
+            cfg = dict(workload=f"C2 post tip, {G} groups x 1024, 2000 panels, rtol 1e-9", groups=G, group_size=1024)
         else:
-            data = w.tip_c4(geo.profile, geo.sigma, seed=4 + rank)
-            cfg = dict(workload="C4 post tip, 65536 groups of size logU[1,128]", groups=65536, group_size="1-128")
-        cfg.update(bem_panels=geo.profile.shape[0] - 1, far_nodes=(geo.profile.shape[0] - 1) * 32)
+            G = 65536 * n_copies
+            data = w.tip_c4(geo.profile, geo.sigma, n_groups=G, seed=4)
+            cfg = dict(workload=f"C4 post tip, {G} groups of size logU[1,128], rtol 1e-9", groups=G,
+                       group_size="1-128")
+        cfg.update(bem_panels=geo.profile.shape[0] - 1, far_nodes=(geo.profile.shape[0] - 1) * 32,
+                   particles=int(np.sum(data["group_sizes"])))
         return dict(geometry=geo, data=data, rtol=1e-9, atol=1e-12, t_max=w.default_t_max(-1e6, 1e-3, 1e-12),
                     z_max=1e-3, config=cfg)
     if name == "c3":
         geo = bg.CylindricalWellBEMGeometry(-2.5e6, 2e-6, 1e-6, n_segments=3000)
-        data = w.well_c3(seed=3 + rank)
+        G = 65536 * n_copies
+        data = w.well_c3(n_groups=G, seed=3)
         return dict(geometry=geo, data=data, rtol=1e-9, atol=1e-12, t_max=w.default_t_max(-2.5e6, 2e-3, 10e-12),
-                    z_max=2e-3, config=dict(workload="C3 cylindrical well, 65536 groups of size logU[1,256]",
-                                            groups=65536, group_size="1-256", bem_panels=geo.profile.shape[0] - 1))
+                    z_max=2e-3, config=dict(workload=f"C3 cylindrical well, {G} groups of size logU[1,256], rtol 1e-9",
+                                            groups=G, group_size="1-256", bem_panels=geo.profile.shape[0] - 1,
+                                            particles=int(np.sum(data["group_sizes"]))))
     raise ValueError(name)
 
 
 def first_groups(data, n):
-    """The workload cut to its first n emission groups (a smaller case of the
-    same kernel, for profiling)."""
-    sizes = np.asarray(data["group_sizes"])
-    if n is None or n >= len(sizes):
+    """The workload cut to its first n emission groups."""
+    from bem_b200.partition import shard
+    if n is None or n >= len(data["group_sizes"]):
         return data
-    k = int(sizes[:n].sum())
-    out = {key: (v[:k] if isinstance(v, np.ndarray) and v.shape[:1] == (int(sizes.sum()),) else v) for key, v in data.items()}
-    out["group_sizes"] = sizes[:n]
-    return out
+    return shard(data, 0, n)
 
 
 def particle_arrays(data):
@@ -111,15 +135,26 @@ def particle_arrays(data):
     return pos, vel, data["t"], np.full(n, -ELEMENTARY_CHARGE), np.full(n, m), -ELEMENTARY_CHARGE / m
 
 
+def _default_t_max(name):
+    from bem_b200 import workloads as w
+    return dict(c0=w.default_t_max(-1e7, 1e-3, 1e-12))[name]
+
+
+def span_t_max(args):
+    """The integrator's t_max for this run: t_end of the trace span."""
+    t = args.t_end if args.t_end is not None else T_END[args.workload]
+    return _default_t_max(args.workload) if t is None else float(t)
+
+
 # ---------------------------------------------------------------------------
 # CPU leg (oracle port; spawn pool, started before any CUDA use)
 
 def _cpu_job(args):
-    name, g, attempts = args
+    g, attempts = args
     import numpy as _np
     from oracle import geometry as ogeo
     from oracle import rk45 as ork
-    wl = build_workload_cpu(name)
+    wl = _cpu_blob()
     data = wl["data"]
     sizes = data["group_sizes"]
     offs = _np.concatenate([[0], _np.cumsum(sizes)])
@@ -134,49 +169,56 @@ def _cpu_job(args):
                                        wl["t_max"], wl["rtol"], wl["atol"],
                                        kill=ogeo.make_kill(spec, wl["z_max"]), max_attempts=attempts)
     dt = time.perf_counter() - t0
-    return int(_np.sum(log[0][2])) * E, len(log[0][0]), dt
+    accepted = int(_np.sum(log[0][2]))
+    return accepted * E, len(log[0][0]), dt
 
 
 _CPU_CACHE = {}
 
 
-def build_workload_cpu(name):
-    """Same workload as build_workload, with the BEM solution taken from the
-    cached device solve (the CPU leg never solves)."""
-    if name in _CPU_CACHE:
-        return _CPU_CACHE[name]
-    blob = np.load(os.environ["SPT_BENCH_CPU_BLOB"], allow_pickle=True)
-    wl = blob["wl"].item()
-    _CPU_CACHE[name] = wl
-    return wl
+def _cpu_blob():
+    path = os.environ["SPT_BENCH_CPU_BLOB"]
+    if path not in _CPU_CACHE:
+        _CPU_CACHE[path] = np.load(path, allow_pickle=True)["wl"].item()
+    return _CPU_CACHE[path]
 
 
-def cpu_leg(name, n_procs, attempts, groups):
+def cpu_leg(n_procs, attempts, groups):
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(n_procs) as pool:
-        res = pool.map(_cpu_job, [(name, g, attempts) for g in groups])
+        res = pool.map(_cpu_job, [(g, attempts) for g in groups])
     wall = time.perf_counter() - t0
     steps = sum(r[0] for r in res)
     return steps / wall, steps, wall, sum(r[1] for r in res)
 
 
-def prepare_cpu_blob(name, wl):
+def _make_blob(name, t_max):
+    wl = build_workload(name)
     spec = wl["geometry"].spec()
-    d = {k: v for k, v in wl["data"].items()}
-    blob = dict(spec=spec, data=d, rtol=wl["rtol"], atol=wl["atol"], t_max=wl["t_max"], z_max=wl["z_max"],
+    blob = dict(spec=spec, data=dict(wl["data"]), rtol=wl["rtol"], atol=wl["atol"], t_max=t_max, z_max=wl["z_max"],
                 config=wl["config"])
     import tempfile
     path = os.path.join(tempfile.gettempdir(), f"spt_bench_cpu_{name}_{os.getpid()}.npz")
     np.savez(path, wl=np.array(blob, dtype=object))
-    os.environ["SPT_BENCH_CPU_BLOB"] = path
     return path
+
+
+def prepare_cpu(name, t_max):
+    """Workload for the CPU legs, built in a spawned child (BEM workloads
+    need the device solve; this process stays CUDA-free for the spawn pool)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        path = pool.apply(_make_blob, (name, t_max))
+    os.environ["SPT_BENCH_CPU_BLOB"] = path
+    return _cpu_blob()
 
 
 def physical_cores():
     """Worker processes for the CPU legs: the physical cores, at most 64, and
-    no more than the available host memory allows at ~1 GiB per worker (a
+    no more than the available host memory allows at ~2 GiB per worker (a
     worker's float64 ring-sum temporaries over 64,000 nodes)."""
     n = os.cpu_count() or 1
     try:
@@ -186,6 +228,25 @@ def physical_cores():
     except Exception:
         pass
     return max(1, min(n, 64))
+
+
+def cpu_sample(wl):
+    procs = min(physical_cores(), 64)
+    groups = list(range(min(procs, len(wl["data"]["group_sizes"]))))
+    return procs, groups
+
+
+def cpu_baseline(args, t_max):
+    """The oracle port on the host cores, on a bounded sample of the same
+    trace: the first `procs` groups (one per process) for --cpu-attempts
+    attempts each from emission, with the same t_max as the GPU span."""
+    wl = prepare_cpu(args.workload, t_max)
+    procs, groups = cpu_sample(wl)
+    value, steps, wall, attempts = cpu_leg(procs, args.cpu_attempts, groups)
+    return dict(value=value, unit=UNIT, cores=procs, kind="port",
+                sample=f"first {len(groups)} groups of the workload, {args.cpu_attempts} attempts each from "
+                       f"emission toward t_max = {t_max:.3g} s (the GPU trace's span), one group per process; "
+                       f"{steps} accepted particle-steps in {wall:.1f} s")
 
 
 # ---------------------------------------------------------------------------
@@ -245,12 +306,9 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # GPU leg
 
-def fp64_peak_tflops(torch, dev):
-    """Measured float64 GEMM rate (cuBLAS DGEMM, 4096^3, best of 5): the
-    FP64 denominator, since the driver's peak file has no FP64 figure."""
-    n = 4096
-    a = torch.randn(n, n, dtype=torch.float64, device=dev)
-    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+def _gemm_peak(torch, dev, dtype, n):
+    a = torch.randn(n, n, dtype=dtype, device=dev)
+    b = torch.randn(n, n, dtype=dtype, device=dev)
     torch.matmul(a, b)
     torch.cuda.synchronize()
     best = 1e30
@@ -265,33 +323,26 @@ def fp64_peak_tflops(torch, dev):
     return 2.0 * n**3 / best / 1e12
 
 
-def fp32_peak_tflops(torch, dev, n=8192):
+def fp64_peak_tflops(torch, dev):
+    """Measured float64 GEMM rate (cuBLAS DGEMM, 4096^3, best of 5): the
+    FP64 denominator (no FP64 figure in the measured-peaks file)."""
+    return _gemm_peak(torch, dev, torch.float64, 4096)
+
+
+def fp32_peak_tflops(torch, dev):
     """Float32 CUDA-core peak measured in-run: a float32 GEMM with TF32 off."""
     old = torch.backends.cuda.matmul.allow_tf32
     torch.backends.cuda.matmul.allow_tf32 = False
     try:
-        a = torch.randn(n, n, dtype=torch.float32, device=dev)
-        b = torch.randn(n, n, dtype=torch.float32, device=dev)
-        torch.matmul(a, b)
-        torch.cuda.synchronize()
-        best = 1e30
-        for _ in range(5):
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record()
-            torch.matmul(a, b)
-            e.record()
-            e.synchronize()
-            best = min(best, s.elapsed_time(e) * 1e-3)
-        del a, b
-        return 2.0 * n**3 / best / 1e12
+        return _gemm_peak(torch, dev, torch.float32, 8192)
     finally:
         torch.backends.cuda.matmul.allow_tf32 = old
 
 
 def combine_ranks(t_total, particle_steps, world, device):
-    """Whole-job numbers of a weak-scaling run: the slowest rank's timed
-    region (max) and the particle-steps of all ranks (sum), by collectives
-    on the initialised process group (NCCL on the GPU path; any backend)."""
+    """Whole-job numbers of a multi-rank run: the slowest rank's timed region
+    (max) and the particle-steps of all ranks (sum), by collectives on the
+    initialised process group (NCCL on the GPU path; any backend)."""
     if world == 1:
         return float(t_total), float(particle_steps)
     import torch
@@ -303,40 +354,104 @@ def combine_ranks(t_total, particle_steps, world, device):
     return float(tt.item()), float(st.item())
 
 
+def make_tracer(args, wl, dev, form=None, far_rule=None):
+    from bem_b200 import engine
+    tr = engine.Tracer(wl["geometry"], device=dev, form=form or args.form, z_max=wl["z_max"],
+                       far_rule=far_rule or args.far_rule)
+    tr.kappa_max = args.kappa
+    return tr
+
+
+class Runner:
+    """One workload on one device: a pristine copy of the initial state, the
+    working batch, and whole-trace (or slice) launches, binned or not."""
+
+    def __init__(self, tracer, pos, vel, tb, q, m, sizes, dev, binned=False):
+        from bem_b200 import engine
+        self.tracer = tracer
+        self.batch = engine.GroupBatch(pos, vel, tb, q, m, sizes, device=dev)
+        self.init = engine.GroupBatch(pos, vel, tb, q, m, sizes, device=dev)
+        self.plan = self.batch.bin_plan() if binned else None
+
+    def reset(self):
+        self.batch.copy_state_from(self.init)
+
+    def launch(self, params, stream):
+        if self.plan is not None:
+            self.tracer.launch_binned(self.batch, params, self.plan, stream)
+        else:
+            self.tracer.launch(self.batch, params, stream)
+
+    def check_done(self):
+        from bem_b200 import engine
+        if not engine.Tracer._check_done(self.batch):
+            raise RuntimeError("a whole-trace launch left groups unfinished")
+
+
 def run_gpu(args, rank, world):
     import torch
-    from bem_b200 import engine
+    from bem_b200 import partition
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
     torch.cuda.set_device(dev)
-    wl = build_workload(args.workload, rank)
+    wl = build_workload(args.workload, n_copies=world)
+    data = wl["data"]
     if args.groups:
-        wl["data"] = first_groups(wl["data"], args.groups)
-        wl["config"] = dict(wl["config"], groups=args.groups, workload=wl["config"]["workload"] + f" (first {args.groups} groups)")
-    pos, vel, tb, q, m, cm = particle_arrays(wl["data"])
-    sizes = wl["data"]["group_sizes"]
-    tracer = engine.Tracer(wl["geometry"], device=dev, form=args.form, z_max=wl["z_max"], far_rule=args.far_rule)
-    tracer.kappa_max = args.kappa
-    batch = engine.GroupBatch(pos, vel, tb, q, m, sizes, device=dev)
+        data = first_groups(data, args.groups * world)
+        wl["config"] = dict(wl["config"], groups=args.groups * world,
+                            workload=wl["config"]["workload"] + f" (first {args.groups * world} groups)")
+    all_sizes = np.asarray(data["group_sizes"])
+    ranges = partition.partition(all_sizes, world)
+    g0, g1 = ranges[rank]
+    local = partition.shard(data, g0, g1)
+    pos, vel, tb, q, m, cm = particle_arrays(local)
+    wl["cm"] = cm
+    sizes = local["group_sizes"]
+    t_max = span_t_max(args)
+    trace = args.span == "trace"
+    budget = WHOLE_TRACE if trace else args.attempts
+
+    tracer = make_tracer(args, wl, dev)
+    if args.cta_threads:
+        tracer.cta_threads = args.cta_threads
     tuned = None
     if args.tune:
-        # launch configuration chosen by the project's autotuner on a sample of this workload (untimed)
         from bem_b200 import autotune
         t0 = time.perf_counter()
-        res = autotune.tune(tracer, pos, vel, tb, q, m, sizes, wl["t_max"], wl["rtol"], wl["atol"], 1e-12, cm)
-        autotune.apply(res, tracer, batch)
-        tracer.tuned_order = res["order"]
+        threads = (args.cta_threads,) if (args.cta_threads or args.bins) else autotune.CTA_THREADS
+        res = autotune.tune(tracer, pos, vel, tb, q, m, sizes, t_max, wl["rtol"], wl["atol"], 1e-12, cm,
+                            threads=threads)
+        autotune.apply(res, tracer)
         args.tuned_config = res
-        tuned = dict(res, seconds=round(time.perf_counter() - t0, 2), sample_groups=res.get("sample_groups"),
+        tuned = dict(res, seconds=round(time.perf_counter() - t0, 2),
                      timings={k: (round(v) if isinstance(v, float) else v) for k, v in res.get("timings", {}).items()})
+    run = Runner(tracer, pos, vel, tb, q, m, sizes, dev, binned=args.bins)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    prm = lambda: tracer.params(wl["t_max"], wl["rtol"], wl["atol"], 1e-12, cm, args.attempts)
+    counts = [int(np.sum(all_sizes[a:b])) for a, b in ranges]
+    gcounts = [b - a for a, b in ranges]
+    prm = lambda: tracer.params(t_max, wl["rtol"], wl["atol"], 1e-12, cm, budget)
+
+    def step():
+        if trace:
+            run.reset()
+        flush.fill_(1.0)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        run.launch(prm(), stream)
+        if world > 1:
+            b = run.batch
+            partition.gather_state({k: getattr(b, k) for k in partition.STATE_PARTICLE + partition.STATE_GROUP},
+                                   counts, gcounts)
+        e.record(stream)
+        e.synchronize()
+        if trace:
+            run.check_done()
+        return s.elapsed_time(e) * 1e-3
 
     for _ in range(args.warmup):
-        tracer.launch(batch, prm(), stream)
+        step()
     torch.cuda.synchronize()
-
     c0 = tracer.counter_dict()
     times = []
     with ClockSampler(dev.index) as clk:
@@ -344,13 +459,7 @@ def run_gpu(args, rank, world):
             torch.distributed.barrier()
         torch.cuda.synchronize()
         for _ in range(args.steps):
-            flush.fill_(1.0)
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record(stream)
-            tracer.launch(batch, prm(), stream)
-            e.record(stream)
-            e.synchronize()
-            times.append(s.elapsed_time(e) * 1e-3)
+            times.append(step())
         torch.cuda.synchronize()
         if world > 1:
             torch.distributed.barrier()
@@ -358,126 +467,120 @@ def run_gpu(args, rank, world):
     dc = {k: c1[k] - c0[k] for k in c1}
     t_total = float(np.sum(times))
     t_max_ranks, steps_all = combine_ranks(t_total, dc["particle_steps"], world, dev)
+    _, live_all = combine_ranks(t_total, dc["live_steps"], world, dev)
 
-    # end-to-end leg: host (pinned) state in, host state out, every step
-    e2e = None
+    e2e = plain = acc = None
     if rank == 0 and not args.no_e2e:
-        e2e = e2e_leg(args, wl, tracer, pos, vel, tb, q, m, cm, sizes, dev)
-
-    plain = None
-    acc = None
+        e2e = e2e_leg(args, wl, tracer, pos, vel, tb, q, m, sizes, dev, t_max, budget)
     if rank == 0 and not args.no_plain and (args.form, args.far_rule) != ("fp64", "reference"):
-        plain = plain_leg(args, wl, pos, vel, tb, q, m, cm, sizes, dev)
-    if rank == 0 and not args.no_accuracy and (args.form, args.far_rule) != ("fp64", "reference"):
-        acc = accuracy_leg(args, wl, pos, vel, tb, q, m, cm, sizes, dev)
+        plain, acc = plain_and_accuracy(args, wl, pos, vel, tb, q, m, sizes, dev, t_max, budget)
     peak = (fp64_peak_tflops if args.form == "fp64" else fp32_peak_tflops)(torch, dev) if rank == 0 else None
     flops = dc["ring_far"] * FLOP_PER_RING + dc["ring_near"] * FLOP_PER_RING + dc["pair_evals"] * FLOP_PER_PAIR
     achieved = flops / t_total / 1e12
-    return dict(value=steps_all / t_max_ranks, t_total=t_max_ranks, times=times, counters=dc, clocks=clk.summary(),
-                e2e=e2e, peak=peak, achieved=achieved, config=wl["config"], wl=wl, plain=plain, accuracy=acc,
-                tuned=tuned)
+    return dict(value=steps_all / t_max_ranks, live=live_all / t_max_ranks, t_total=t_max_ranks, times=times,
+                counters=dc, clocks=clk.summary(), e2e=e2e, peak=peak, achieved=achieved, config=wl["config"],
+                plain=plain, accuracy=acc, tuned=tuned, t_max=t_max, ranges=ranges,
+                launches_per_step=len(run.plan) if run.plan else 1)
 
 
-def plain_leg(args, wl, pos, vel, tb, q, m, cm, sizes, dev):
-    """The plain form (float64, the reference's far quadrature) on the same
-    workload: the same W warm-up and K timed steps, CUDA events."""
+def plain_and_accuracy(args, wl, pos, vel, tb, q, m, sizes, dev, t_max, budget):
+    """The plain form (float64, the reference's quadrature) and the chosen
+    form over the same span on the first --plain-groups groups: the ratio of
+    their rates, and the chosen form's endpoint error against the plain one
+    (alive particles by position and velocity; particles killed at the
+    emitter or at z_max keep the state of the step that crossed, which moves
+    with the step sequence: compared by death time)."""
     import torch
-    from bem_b200 import engine
-
-    tracer = engine.Tracer(wl["geometry"], device=dev, form="fp64", z_max=wl["z_max"], far_rule="reference")
-    batch = engine.GroupBatch(pos, vel, tb, q, m, sizes, device=dev)
+    n = min(args.plain_groups, len(sizes))
+    k = int(np.sum(sizes[:n]))
+    sub = (pos[:k], vel[:k], tb[:k], q[:k], m[:k], sizes[:n])
+    out = {}
     stream = torch.cuda.current_stream(dev)
-    prm = lambda: tracer.params(wl["t_max"], wl["rtol"], wl["atol"], 1e-12, cm, args.attempts)
-    for _ in range(args.warmup):
-        tracer.launch(batch, prm(), stream)
-    torch.cuda.synchronize()
-    c0 = tracer.counter_dict()
-    t = 0.0
-    for _ in range(args.steps):
+    for name, form, rule in (("plain", "fp64", "reference"), ("chosen", args.form, args.far_rule)):
+        tracer = make_tracer(args, wl, dev, form, rule)
+        binned = False
+        if name == "chosen":
+            binned = args.bins
+            if getattr(args, "tuned_config", None):
+                from bem_b200 import autotune
+                autotune.apply(args.tuned_config, tracer)
+            elif args.cta_threads:
+                tracer.cta_threads = args.cta_threads
+        run = Runner(tracer, *sub, dev, binned=binned)
+        prm = lambda a: tracer.params(t_max, wl["rtol"], wl["atol"], 1e-12, wl["cm"], a)
+        # warm-up: a short slice, then the timed span from the initial state
+        run.launch(prm(4), stream)
+        torch.cuda.synchronize()
+        run.reset()
+        c0 = tracer.counter_dict()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
-        tracer.launch(batch, prm(), stream)
+        run.launch(prm(budget), stream)
         e.record(stream)
         e.synchronize()
-        t += s.elapsed_time(e) * 1e-3
-    steps = tracer.counter_dict()["particle_steps"] - c0["particle_steps"]
-    return dict(value=steps / t, unit=UNIT, ms_per_step=1e3 * t / args.steps, form="fp64", far_rule="reference")
-
-
-def accuracy_leg(args, wl, pos, vel, tb, q, m, cm, sizes, dev):
-    """Endpoint error of the chosen form against the plain form: the first
-    `acc_groups` groups traced to t_end = acc_time by both (a fixed end time,
-    so no endpoint depends on which step crossed z_max).  Particles alive at
-    t_end: |dx| / |x| and |dv| / |v| of the plain endpoint.  Particles that
-    returned to the emitter keep the state of the step that landed inside it,
-    which moves with the step sequence: they are compared by death time."""
-    import torch
-    from bem_b200 import engine
-
-    n = min(args.acc_groups, len(sizes))
-    k = int(np.sum(sizes[:n]))
-    out = {}
-    for form, rule in (("fp64", "reference"), (args.form, args.far_rule)):
-        tracer = engine.Tracer(wl["geometry"], device=dev, form=form, z_max=wl["z_max"], far_rule=rule)
-        tracer.kappa_max = args.kappa
-        batch = engine.GroupBatch(pos[:k], vel[:k], tb[:k], q[:k], m[:k], sizes[:n], device=dev)
-        if (form, rule) == (args.form, args.far_rule) and getattr(args, "tuned_config", None):
-            from bem_b200 import autotune
-            autotune.apply(args.tuned_config, tracer, batch)  # the chosen form as timed
-        tracer.run(batch, args.acc_time, wl["rtol"], wl["atol"], 1e-12, cm)
-        torch.cuda.synchronize()
-        c = tracer.counter_dict()
-        out[form, rule] = (batch.positions().cpu().numpy(), batch.velocities().cpu().numpy(),
-                           batch.t_death.cpu().numpy(), c["attempts"], c["accepted"])
-    (p0, v0, d0, a0, s0), (p1, v1, d1, a1, s1) = out[("fp64", "reference")], out[(args.form, args.far_rule)]
+        c = {kk: v - c0[kk] for kk, v in tracer.counter_dict().items()}
+        b = run.batch
+        out[name] = dict(t=s.elapsed_time(e) * 1e-3, c=c, pos=b.positions().cpu().numpy(),
+                         vel=b.velocities().cpu().numpy(), td=b.t_death.cpu().numpy())
+    P, C = out["plain"], out["chosen"]
+    rate = lambda o: o["c"]["particle_steps"] / o["t"]
+    span = f"whole trace to t = {t_max:.3g} s" if budget == WHOLE_TRACE else f"{budget} attempts from emission"
+    plain = dict(value=rate(P), unit=UNIT, seconds=P["t"], form="fp64", far_rule="reference", groups=n,
+                 chosen_value_same_groups=rate(C), chosen_seconds=C["t"], ratio=rate(C) / rate(P),
+                 time_ratio=P["t"] / C["t"], span=f"first {n} groups, {span}")
+    d0, d1 = P["td"], C["td"]
     alive = ~np.isfinite(d0) & ~np.isfinite(d1)
     dead = np.isfinite(d0) & np.isfinite(d1)
-    ex = np.linalg.norm(p1 - p0, axis=-1)[alive] / np.linalg.norm(p0, axis=-1)[alive]
-    ev = np.linalg.norm(v1 - v0, axis=-1)[alive] / np.linalg.norm(v0, axis=-1)[alive]
+    ex = np.linalg.norm(C["pos"] - P["pos"], axis=-1)[alive] / np.linalg.norm(P["pos"], axis=-1)[alive]
+    ev = np.linalg.norm(C["vel"] - P["vel"], axis=-1)[alive] / np.linalg.norm(P["vel"], axis=-1)[alive]
     et = np.abs(d1[dead] - d0[dead]) / d0[dead]
-    return dict(groups=n, particles=k, t_end=args.acc_time, against="plain fp64 (reference quadrature) on the GPU",
-                alive=int(alive.sum()), max_rel_pos=float(ex.max()), median_rel_pos=float(np.median(ex)),
-                max_rel_vel=float(ev.max()), median_rel_vel=float(np.median(ev)),
-                killed=int(dead.sum()), killed_in_one_only=int((np.isfinite(d0) != np.isfinite(d1)).sum()),
-                max_rel_t_death=float(et.max()) if et.size else None,
-                attempts_plain=int(a0), attempts_chosen=int(a1), accepted_steps_ratio=float(s1 / s0))
+    acc = dict(groups=n, particles=k, t_end=t_max, against="plain fp64 (reference quadrature) on the GPU",
+               alive=int(alive.sum()), max_rel_pos=float(ex.max()) if ex.size else None,
+               median_rel_pos=float(np.median(ex)) if ex.size else None,
+               max_rel_vel=float(ev.max()) if ev.size else None,
+               killed=int(dead.sum()), killed_in_one_only=int((np.isfinite(d0) != np.isfinite(d1)).sum()),
+               max_rel_t_death=float(et.max()) if et.size else None,
+               attempts_plain=int(P["c"]["attempts"]), attempts_chosen=int(C["c"]["attempts"]),
+               accepted_steps_ratio=float(C["c"]["accepted"] / max(P["c"]["accepted"], 1)))
+    return plain, acc
 
 
-def e2e_leg(args, wl, tracer, pos, vel, tb, q, m, cm, sizes, dev):
-    """Same slices through the public API with the state in pinned host
-    memory: H2D of the step's state, spt_trace, D2H of the new state."""
+def e2e_leg(args, wl, tracer, pos, vel, tb, q, m, sizes, dev, t_max, budget):
+    """The same traces through the public API with the state in pinned host
+    memory: every step copies the initial state host -> device, traces, and
+    copies the final state device -> host.  min(K, 3) steps after one
+    warm-up."""
     import torch
     from bem_b200 import engine
 
-    batch = engine.GroupBatch(pos, vel, tb, q, m, sizes, device=dev)
-    if getattr(tracer, "tuned_order", None):
-        batch.set_order(tracer.tuned_order)
-    names = ["x", "y", "z", "vx", "vy", "vz", "t_death", "t", "h", "status", "n_accepted", "n_rejected"]
-    host = {k: torch.empty_like(getattr(batch, k), device="cpu").pin_memory() for k in names}
+    run = Runner(tracer, pos, vel, tb, q, m, sizes, dev, binned=args.bins)
+    batch = run.batch
+    names = list(engine.GroupBatch.STATE)
+    host_in = {k: torch.empty_like(getattr(batch, k), device="cpu").pin_memory() for k in names}
+    host_out = {k: torch.empty_like(getattr(batch, k), device="cpu").pin_memory() for k in names}
     for k in names:
-        host[k].copy_(getattr(batch, k))
+        host_in[k].copy_(getattr(batch, k))
     stream = torch.cuda.current_stream(dev)
-    prm = lambda: tracer.params(wl["t_max"], wl["rtol"], wl["atol"], 1e-12, cm, args.attempts)
-    for _ in range(args.warmup):
-        tracer.launch(batch, prm(), stream)
-    torch.cuda.synchronize()
-    for k in names:
-        host[k].copy_(getattr(batch, k))
-    h2d = sum(host[k].numel() * host[k].element_size() for k in names)
-    c0 = tracer.counter_dict()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
+    prm = lambda: tracer.params(t_max, wl["rtol"], wl["atol"], 1e-12, wl["cm"], budget)
+    nbytes = sum(host_in[k].numel() * host_in[k].element_size() for k in names)
+    n_steps = max(1, min(args.steps, 3))
+    c_total, wall = 0, 0.0
+    for it in range(1 + n_steps):
+        c0 = tracer.counter_dict()["particle_steps"]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         for k in names:
-            getattr(batch, k).copy_(host[k], non_blocking=True)
-        tracer.launch(batch, prm(), stream)
+            getattr(batch, k).copy_(host_in[k], non_blocking=True)
+        run.launch(prm(), stream)
         for k in names:
-            host[k].copy_(getattr(batch, k), non_blocking=True)
+            host_out[k].copy_(getattr(batch, k), non_blocking=True)
         stream.synchronize()
-    wall = time.perf_counter() - t0
-    c1 = tracer.counter_dict()
-    steps = c1["particle_steps"] - c0["particle_steps"]
-    return dict(value=steps / wall, unit=UNIT, h2d_bytes_per_step=int(h2d), d2h_bytes_per_step=int(h2d))
+        dt = time.perf_counter() - t0
+        if it > 0:
+            wall += dt
+            c_total += tracer.counter_dict()["particle_steps"] - c0
+    return dict(value=c_total / wall, unit=UNIT, h2d_bytes_per_step=int(nbytes), d2h_bytes_per_step=int(nbytes),
+                steps=n_steps)
 
 
 def load_traffic(workload, form, far_rule):
@@ -498,21 +601,26 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c1", choices=["c0", "c1", "c2", "c3", "c4"])
-    ap.add_argument("--attempts", type=int, default=16, help="RK45 attempts per group per step")
+    ap.add_argument("--span", default="trace", choices=["trace", "slice"],
+                    help="trace: a step is a whole trace from emission to t_end; slice: --attempts per group")
+    ap.add_argument("--t-end", type=float, default=None, help="end of the trace span [s] (default per workload)")
+    ap.add_argument("--attempts", type=int, default=16, help="--span slice: RK45 attempts per group per step")
     ap.add_argument("--form", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--far-rule", default="adaptive", choices=["reference", "adaptive"],
                     help="far-field quadrature of the BEM sum (adaptive: whole-segment Gauss-4/2 when distant)")
+    ap.add_argument("--cta-threads", type=int, default=0, help="CTA width (0: autotuned, or the library's choice)")
+    ap.add_argument("--bins", action="store_true",
+                    help="size-binned scheduling: one launch per group-size bin on concurrent streams")
     ap.add_argument("--cpu-attempts", type=int, default=16)
-    ap.add_argument("--groups", type=int, default=None, help="first N emission groups only (profiling a smaller case)")
-    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain form beside the chosen one")
+    ap.add_argument("--groups", type=int, default=None, help="first N emission groups only (a smaller case)")
+    ap.add_argument("--plain-groups", type=int, default=592,
+                    help="groups traced by both forms for the ratio and the endpoint error")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-form and accuracy leg")
     ap.add_argument("--tune", dest="tune", action="store_true", default=True,
                     help="autotune the launch configuration first (untimed; the default)")
     ap.add_argument("--no-tune", dest="tune", action="store_false", help="time the default launch configuration")
     ap.add_argument("--kappa", type=float, default=0.0,
                     help="mixed form: conditioning bound above which float32 sums are redone in float64 (0: 16)")
-    ap.add_argument("--no-accuracy", action="store_true", help="skip the endpoint-error leg")
-    ap.add_argument("--acc-groups", type=int, default=64)
-    ap.add_argument("--acc-time", type=float, default=20e-12, help="end time of the endpoint-error traces [s]")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
@@ -525,7 +633,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(args)
+        cpu = cpu_baseline(args, span_t_max(args))
 
     if world > 1:
         import torch
@@ -541,26 +649,28 @@ def main():
     t = load_traffic(args.workload, args.form, args.far_rule)
     mean_ms = 1e3 * r["t_total"] / args.steps
     fp64 = args.form == "fp64"
-    plain = r["plain"]
-    if plain is not None:
-        plain = dict(plain, ratio=r["value"] / plain["value"])
+    span = (f"whole trace: every group from emission to t_end = {r['t_max']:.3g} s (integrator t_max), one launch "
+            f"{'per size bin ' if args.bins else ''}per step, initial state restored untimed"
+            if args.span == "trace" else f"slices of {args.attempts} attempts per group per step, continuing")
     line = dict(
         metric=METRIC, value=r["value"], unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
         ms_per_step=mean_ms, higher_is_better=True, scaling="weak", vs_baseline=None,
         dtype="f64" if fp64 else "f32+f64", data="synthetic (seeded samplers, workloads.py)",
-        config=dict(r["config"], form=args.form, far_rule=args.far_rule, attempts_per_step=args.attempts,
-                    kappa_max=args.kappa or 16.0, autotuned=r["tuned"],
-                    parallelism=f"groups x {world} GPUs",
+        config=dict(r["config"], form=args.form, far_rule=args.far_rule, span=span, t_end=r["t_max"],
+                    kappa_max=args.kappa or 16.0, autotuned=r["tuned"], size_binned=bool(args.bins),
+                    cta_threads=(r["tuned"] or {}).get("cta_threads") or args.cta_threads or "library default",
+                    parallelism=f"contiguous group ranges balanced by cost, {world} GPU(s)",
                     l2="flushed between steps (256 MiB write); each step timed alone with CUDA events"),
-        clocks=r["clocks"], gpu_launches=args.steps,
+        live_particle_steps_per_s=r["live"],
+        clocks=r["clocks"], gpu_launches=args.steps * r["launches_per_step"],
         roofline=dict(bound="fp64" if fp64 else "fp32", achieved=r["achieved"], peak=r["peak"], unit="TFLOP/s",
                       frac=(r["achieved"] / r["peak"]) if r["peak"] else None,
                       traffic=(t or {}).get("dram_bytes_per_launch"),
                       peak_source=("measured in-run: cuBLAS DGEMM 4096^3" if fp64 else
                                    "measured in-run: cuBLAS SGEMM 8192^3, TF32 off")
-                      + " (the driver's peak file has HBM and BF16 figures only)",
+                      + " (no FP32/FP64 figure in the measured-peaks file)",
                       flop_model=f"{FLOP_PER_RING:g} FLOP/ring eval, {FLOP_PER_PAIR:g} FLOP/pair (nominal)"),
-        plain_fp64=plain,
+        plain_fp64=r["plain"],
         accuracy=r["accuracy"],
         counters=r["counters"],
         e2e=r["e2e"],
@@ -570,61 +680,33 @@ def main():
     return 0
 
 
-def cpu_baseline(args, for_reference=False):
-    """The oracle port on the host cores, on a bounded sample of the same
-    workload: `procs` groups (one per process) for --cpu-attempts attempts each
-    from the initial state."""
-    wl = build_workload_cpu_side(args.workload)
-    procs = min(physical_cores(), 64)
-    n_groups = len(wl["data"]["group_sizes"])
-    groups = list(range(min(procs, n_groups)))
-    value, steps, wall, attempts = cpu_leg(args.workload, procs, args.cpu_attempts, groups)
-    return dict(value=value, unit=UNIT, cores=procs, kind="port",
-                sample=f"{len(groups)} groups x {args.cpu_attempts} attempts from emission, one group per process "
-                       f"({steps} accepted particle-steps in {wall:.1f} s)")
-
-
-def build_workload_cpu_side(name):
-    """Build the workload for the CPU leg without touching CUDA for the
-    non-BEM case; BEM workloads need the device solve, done in a child
-    process so this process stays CUDA-free for the spawn pool."""
-    import multiprocessing as mp
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(1) as pool:
-        path = pool.apply(_make_blob, (name,))
-    os.environ["SPT_BENCH_CPU_BLOB"] = path
-    return build_workload_cpu(name)
-
-
-def _make_blob(name):
-    wl = build_workload(name)
-    return prepare_cpu_blob(name, wl)
-
-
 def reference_arm(args, rank, world):
     """The reference's algorithm for this path on the host cores (the NumPy
-    oracle port, float64, the reference's quadrature), on the same workload:
-    each step is a bounded sample -- one group per process, --cpu-attempts
-    attempts from emission.  Under torchrun only rank 0 runs."""
+    oracle port, float64, the reference's quadrature), on the same workload
+    and trace span (t_max = t_end): each step is a bounded sample -- the first
+    `procs` groups, one per process, --cpu-attempts attempts each from
+    emission.  Under torchrun only rank 0 runs."""
     if rank != 0:
         return 0
-    wl = build_workload_cpu_side(args.workload)
-    procs = min(physical_cores(), 64)
-    groups = list(range(min(procs, len(wl["data"]["group_sizes"]))))
+    t_max = span_t_max(args)
+    wl = prepare_cpu(args.workload, t_max)
+    procs, groups = cpu_sample(wl)
     total_steps, total_wall = 0, 0.0
     for _ in range(args.steps):
-        value, steps, wall, _ = cpu_leg(args.workload, procs, args.cpu_attempts, groups)
+        value, steps, wall, _ = cpu_leg(procs, args.cpu_attempts, groups)
         total_steps += steps
         total_wall += wall
     value = total_steps / total_wall
     cpu = dict(value=value, unit=UNIT, cores=procs, kind="port",
-               sample=f"per step {len(groups)} groups x {args.cpu_attempts} attempts from emission, one group per "
-                      f"process; {args.steps} steps, {total_steps} accepted particle-steps in {total_wall:.1f} s")
+               sample=f"per step the first {len(groups)} groups, {args.cpu_attempts} attempts each from emission "
+                      f"toward t_max = {t_max:.3g} s, one group per process; {args.steps} steps, {total_steps} "
+                      f"accepted particle-steps in {total_wall:.1f} s")
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=0,
                 ms_per_step=1e3 * total_wall / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
                 dtype="f64", data="synthetic (seeded samplers, workloads.py)", impl="reference",
-                config=dict(wl.get("config", {}), form="fp64 (reference algorithm, NumPy port)",
-                            attempts_per_step=args.cpu_attempts),
+                config=dict(wl.get("config", {}), form="fp64 (reference algorithm, NumPy port)", t_end=t_max,
+                            span=f"{args.cpu_attempts} attempts per group from emission (a bounded prefix of the "
+                                 f"GPU arm's whole trace)"),
                 cpu_baseline=cpu, e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line))
     return 0

@@ -21,6 +21,18 @@ from bem_b200.tables import BemTables  # noqa: E402
 import gpu_util as gu  # noqa: E402
 
 
+def test_elliptic_float32_matches_scipy():
+    """Float32 K(1-p), E(1-p): the DLMF 19.12 series below p = 1e-2, the
+    Hastings approximations (A&S 17.3.34 / 17.3.36, |error| <= 2e-8) above;
+    against SciPy's values recorded by the reference, within float32
+    rounding (5e-7 relative) for p in [1e-6, 1]."""
+    g = load_golden("ellip")
+    sel = (g["p"] >= 1e-6)
+    K, E = engine.ellip_ke(g["p"][sel], form="mixed")
+    np.testing.assert_allclose(K.cpu().numpy(), g["K"][sel], rtol=5e-7, atol=0)
+    np.testing.assert_allclose(E.cpu().numpy(), g["E"][sel], rtol=5e-7, atol=0)
+
+
 @pytest.mark.parametrize("fixture", ["bem_sphere", "bem_well", "bem_post"])
 def test_bem_field_mixed(fixture):
     g = load_golden(fixture)

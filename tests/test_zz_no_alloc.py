@@ -82,6 +82,33 @@ def test_noalloc_matches_trace_large_groups_two_calls():
     _two_calls(spec, pos, vel, d["t"], [300] * 3, w.default_t_max(-1e7, 1e-3, 1e-12), 1e-8, 1e-3, 6)
 
 
+def test_noalloc_more_groups_than_scratch_slots_two_calls():
+    """12 groups of 1024 particles: the scratch holds 9 slope buffers of
+    that size, so the persistent grid is capped at 9 CTAs and the work
+    queue hands the other 3 groups to CTAs that finished (and 40 groups of
+    300 against 32 buffers)."""
+    from bem_b200 import workloads as w
+    spec = dict(kind="flat", E_gun=-1e7, z0=3e-9, kill_z_below=0.0)
+    for n_groups, E, attempts in ((12, 1024, 3), (40, 300, 4)):
+        d = w.flat_c0(n_groups=n_groups, n_emit=E, seed=10, t_spread=2e-15)
+        pos = np.stack([d["x"], d["y"], d["z"]], -1)
+        vel = np.stack([d["px"], d["py"], d["pz"]], -1) * gu.ophys.ELEMENTARY_CHARGE / gu.ophys.SPEED_OF_LIGHT / gu.M_E
+        _two_calls(spec, pos, vel, d["t"], [E] * n_groups, w.default_t_max(-1e7, 1e-3, 1e-12), 1e-8, 1e-3, attempts)
+
+
+def test_noalloc_rejects_the_learned_form():
+    s = _lib.SptState()
+    s.n_groups = 1
+    s.max_group_size = 8
+    p = _lib.SptTraceParams()
+    p.form = _lib.FORM_SURROGATE
+    g = _lib.SptGeometry()
+    g.kind = _lib.GEOM_POST_BEM
+    rc = _lib.lib().spt_trace_noalloc(ctypes.byref(s), ctypes.byref(p), ctypes.byref(g), None, None)
+    assert rc == _lib.SPT_ERR_ARG
+    assert "learned form is not offered" in _lib.last_error()
+
+
 def test_noalloc_rejects_groups_above_limit():
     s = _lib.SptState()
     s.n_groups = 1
