@@ -6,7 +6,10 @@ Checks: the in-kernel network agrees with the standalone one
 (FieldSurrogate.predict); with every point exact (band covering all, or
 spot = 1) the learned form reproduces the mixed form; a trace
 driven by the surrogate stays close to the exact one and does a fraction of
-its ring evaluations (the ablation)."""
+its ring evaluations (the ablation); and, trained at the full learned-form
+specification on the C1 tip, the measured comparison with the chosen form
+on C4-sized groups (time to the same end time, attempts, endpoint error
+against the plain float64 form)."""
 
 import numpy as np
 import pytest
@@ -180,3 +183,61 @@ def test_surrogate_points_drive_the_trace(post):
           f"attempts {c['attempts']} vs {c_ref['attempts']}; ring evals per stage {per_stage(c):.0f} vs {per_stage(c_ref):.0f}")
     assert rel < 0.5, rel
     assert per_stage(c) < 0.5 * per_stage(c_ref)
+
+
+def test_learned_form_measured_against_chosen_form():
+    """The learned form at its full specification (4 x 128 SiLU MLP, BF16;
+    2M training points log-uniform 1 nm - 1 mm from the surface, labelled by
+    the float64 BEM evaluator; Adam, lr 1e-3 cosine, 20k steps, batch 8192;
+    exact BEM within 5 nm, 1 % spot checks) on the C1 tip, against the chosen
+    form (float32 + Kahan, adaptive far rule, no network), both tracing 148
+    C4-sized groups (sizes logU[1, 128], seed 4) to t = 0.1 ps.  Measured:
+    CUDA-event time to reach t_end, attempts, accepted particle-steps and the
+    endpoint error against the plain float64 form.  Particle-steps per second
+    alone would reward a form that takes more, smaller steps, so the verdict
+    is on time to the same end time at <= 1e-6 endpoint error.
+
+    What this measures (printed): the network replaces most ring
+    evaluations, but its BF16 output is not smooth at the 1e-9 level the
+    rtol = 1e-9 controller resolves, so the controller takes far more steps
+    and the endpoints miss 1e-6 -- the learned form does not beat the chosen
+    form.  This test asserts that finding; a network that changes it makes
+    the test fail, and the chosen form should then be revisited."""
+    from bem_b200 import geometry as bg, workloads as w
+    g = load_golden("sigma_c1")
+    geo = bg.PostTipBEMGeometry(-1e6, 50e-9, 5e-6, profile=g["profile"], sigma=g["sigma"])
+    model = sg.train(geo, seed=4)  # the full specification (the defaults)
+    d = w.tip_c4(geo.profile, geo.sigma, n_groups=148, seed=4)
+    pos = np.stack([d["x"], d["y"], d["z"]], -1)
+    vel = np.stack([d[k] for k in ("px", "py", "pz")], -1) * (gu.ophys.ELEMENTARY_CHARGE / gu.ophys.SPEED_OF_LIGHT
+                                                              / gu.M_E)
+    n = len(pos)
+    t_end = 0.1e-12
+    out = {}
+    for name, form, rule, kw in (("plain", "fp64", "reference", {}), ("chosen", "mixed", "adaptive", {}),
+                                 ("learned", "surrogate", "adaptive", dict(surrogate=model, band=5e-9, spot=0.01))):
+        tr = engine.Tracer(geo, form=form, far_rule=rule, z_max=1e-3, **kw)
+        b = engine.GroupBatch(pos, vel, d["t"], np.full(n, gu.Q_E), np.full(n, gu.M_E), d["group_sizes"])
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        tr.run(b, t_end, 1e-9, 1e-12, 1e-12, gu.CM, max_steps=2_000_000, attempt_chunk=2_000_000)
+        e.record()
+        e.synchronize()
+        out[name] = dict(t=s.elapsed_time(e) * 1e-3, c=tr.counter_dict(), pos=b.positions().cpu().numpy(),
+                         td=b.t_death.cpu().numpy())
+    ref = out["plain"]
+    alive = np.isinf(ref["td"])
+    for name in ("chosen", "learned"):
+        o = out[name]
+        ok = alive & np.isinf(o["td"])
+        o["err"] = float((np.linalg.norm(o["pos"] - ref["pos"], axis=-1)[ok] /
+                          np.linalg.norm(ref["pos"], axis=-1)[ok]).max())
+        c = o["c"]
+        o["per_stage"] = (c["ring_far"] + c["ring_near"]) / max(1, c["stage_evals"])
+        print(f"{name}: {o['t']:.3f} s to t_end, {c['attempts']} attempts, {c['particle_steps']} particle-steps "
+              f"({c['particle_steps'] / o['t']:.3e}/s), ring evals per stage {o['per_stage']:.0f}, "
+              f"max endpoint error vs plain {o['err']:.2e}")
+    C, L = out["chosen"], out["learned"]
+    assert C["err"] <= 1e-6                         # the chosen form meets the bar
+    assert L["per_stage"] < 0.5 * C["per_stage"]    # the network does replace most ring evaluations ...
+    assert L["err"] > 1e-6 or L["t"] > C["t"]       # ... but does not beat the chosen form within 1e-6
