@@ -116,8 +116,11 @@ TRACE_RTOL = dict(trace_flat=1e-6, trace_flat_c0=1e-6, trace_tip=1e-7, trace_tip
 # reference's on-surface threshold dist^2 < (1e-9 L)^2 or just outside it
 # depending on the last ulp, and the field is evaluated at the 1e-4 L offset
 # point in one case and not in the other.  Early step sizes then differ by
-# up to 1e-4 (the decisions stay identical).
-T_ACC_RTOL = dict(trace_well=1e-3)
+# up to 1e-4 (the decisions stay identical).  trace_tip_bem, the fixture
+# whose endpoints move 1.4e-7 under a 1e-15 change of its inputs, has step
+# times within 2.3e-6 once the far sums take rounds of 4 points (the
+# summation order): checked at 1e-5, its endpoint tolerance.
+T_ACC_RTOL = dict(trace_well=1e-3, trace_tip_bem=1e-5)
 
 
 @pytest.mark.parametrize("name", sorted(TRACE_RTOL))
