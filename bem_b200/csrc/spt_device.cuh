@@ -965,8 +965,10 @@ __device__ __forceinline__ void bem_sums(Ctx& c, int n, int* status_flag) {
             __syncthreads();
             if (redo) {
                 if (tid == 0) atomicAdd(c.cnt + SPT_CNT_FP64_ROUNDS, 1ull);
-                // rare: one tile shape serves every round size
-                far_pass<4, 2, false, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                // the tile shape the float64 form takes for this round size (same sums, bit for bit)
+                if (np_ == 1) far_pass<1, 8, false, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                else if (np_ == 2) far_pass<2, 4, false, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                else far_pass<4, 2, false, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
             }
         }
     }
