@@ -173,7 +173,7 @@ struct Layout {
     int img;                  // 4E sphere images
     int bpt;                  // 8E per BEM list entry: x y z rho_e z_e near_r near_z (+1 pad)
     int sur;                  // surrogate region: act (4096), wt (4096), sout 2E, sseg E, st E, sd E, feat 128; -1 if none
-    int tiles;                // reference far rule: 2 * 3 * tile_cap node tiles; adaptive: 3 * kAdaptSegs segment lists
+    int tiles;                // reference far rule: 2 * 3 * tile_cap node tiles; adaptive: per-warp scratch
     int tile_cap;             // nodes per TMA tile row (reference far rule)
     int red;                  // kMaxWarps * 3 * kRound (far-round reduction: E_rho, E_z, sum of |terms|)
     int ints;                 // int region start (in doubles)
@@ -183,16 +183,22 @@ struct Layout {
     bool big;                 // slopes/y0/nw in global memory
 };
 
-// Segments per chunk of the adaptive far rule (16 runs of SPT_BLOCK_SEGS);
-// its three segment lists take 3 * kAdaptSegs ints of shared memory.
-constexpr int kAdaptSegs = 512;
+// Segments per chunk of the adaptive far rule (8 runs of SPT_BLOCK_SEGS).
+// Each warp classifies and sums its own rounds in a private scratch of
+// kWarpScratchInts ints: three segment lists of kWarpChunk entries, the
+// near masks of the first (kWarpChunk bytes) and four run lists.
+constexpr int kWarpChunk = 256;
+constexpr int kWarpScratchInts = 3 * kWarpChunk + kWarpChunk / 4 + 4 * (kWarpChunk / SPT_BLOCK_SEGS);
+static_assert(kWarpScratchInts % 2 == 0, "per-warp scratch keeps 8-byte alignment");
 
 // Shared-memory layout of one CTA for groups of up to E particles.  The far
 // rule decides the big region: node tiles for the reference rule (the TMA
 // bulk engine streams the node table through them), segment lists for the
-// adaptive rule (which reads its few nodes through L1/L2).  want_tiles
-// false: neither (paths that evaluate no far sum).
-__host__ __device__ inline Layout make_layout(int E, int far_rule, bool want_sur = false, bool want_tiles = true) {
+// adaptive rule (which reads its few nodes through L1/L2), one scratch per
+// warp of a CTA of `warps` warps.  want_tiles false: neither (paths that
+// evaluate no far sum).
+__host__ __device__ inline Layout make_layout(int E, int far_rule, bool want_sur = false, bool want_tiles = true,
+                                              int warps = kMaxWarps) {
     Layout L;
     const bool big = E > kSmallGroup;
     int o = 0;
@@ -228,7 +234,7 @@ __host__ __device__ inline Layout make_layout(int E, int far_rule, bool want_sur
     for (int cap = kTileNodes; cap >= 256; cap >>= 1) {
         o = base;
         L.tile_cap = tiles ? cap : 0;
-        L.tiles = o; o += tiles ? 2 * 3 * cap : (lists ? 3 * kAdaptSegs / 2 : 0);
+        L.tiles = o; o += tiles ? 2 * 3 * cap : (lists ? warps * kWarpScratchInts / 2 : 0);
         L.red = o; o += kMaxWarps * 3 * kRound;
         L.ints = o;
         L.total_doubles = o + (n_ints + 1) / 2;
@@ -293,7 +299,7 @@ __device__ inline void bind(Ctx& c, double* smem, int E, int far_rule, double* s
     c.E = E;
     c.nt = blockDim.x;
     c.nw = blockDim.x >> 5;
-    c.L = make_layout(E, far_rule, sur);
+    c.L = make_layout(E, far_rule, sur, true, blockDim.x >> 5);
     c.round_pts = kRound;
     c.kappa = kKappa;
     c.cnt = s_cnt;
@@ -558,39 +564,38 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
     round_reduce<NP, MIX>(c, r0, np_, ar, az, fr, fz, kr, kz, sa);
 }
 
-// Adaptive far sum (SPT_FAR_ADAPTIVE) for points r0..r0+np_-1 of the list.
-// Segments are taken kAdaptSegs at a time (32 runs of SPT_BLOCK_SEGS).  One
-// warp classifies the chunk's runs by the smallest lower-bound distance over
-// the round's points: flagged runs at least ratio_run arclengths away take
-// the 8-point rule over the whole run (list R3), runs whose every segment is
-// at least ratio2 lengths away take Gauss-2 on each segment (R2), the rest
-// (M) are classified segment by segment -- below ratio4 lengths the
-// reference nodes, with an 8-bit mask of the points for which the segment is
-// near (they skip it), below ratio2 Gauss-4, else Gauss-2 (lists L0, L1, L2,
-// in the TMA tile region, which this rule does not use).  The flattened node
-// list L0 | L1 | L2 | R2 | R3 is then evaluated like far_round's tiles,
-// nodes read through L1/L2.  Without run bounds every run is in M.
-constexpr int kAdaptRuns = kAdaptSegs / SPT_BLOCK_SEGS;
-static_assert(kAdaptRuns <= 32, "one warp classifies a chunk's runs");
-static_assert(kAdaptSegs <= kRound * 256, "near masks must fit the near-flag bytes");
-static_assert(160 <= kMaxWarps * 3 * kRound * 2, "run lists and counts fit the reduction scratch");
+// Adaptive far sum (SPT_FAR_ADAPTIVE) for points r0..r0+np_-1 of the list,
+// computed by ONE warp (each warp of the CTA takes its own rounds; nothing
+// here waits on another warp).  Segments are taken kWarpChunk at a time
+// (kWarpRuns runs of SPT_BLOCK_SEGS).  The warp classifies the chunk's runs by
+// the smallest lower-bound distance over the round's points: flagged runs at
+// least ratio_run arclengths away take the 8-point rule over the whole run
+// (list R3), runs whose every segment is at least ratio2 lengths away take
+// Gauss-2 on each segment (R2), the rest (M) are classified segment by
+// segment -- below ratio4 lengths the reference nodes, with an 8-bit mask of
+// the points for which the segment is near (they skip it), below ratio2
+// Gauss-4, else Gauss-2 (lists L0, L1, L2 in the warp's own shared scratch).
+// The flattened node list L0 | L1 | L2 | R2 | R3 is then evaluated by the
+// warp's lanes, NQ nodes in flight per lane, nodes read through L1/L2.
+// Without run bounds every run is in M.  Lane 0 ends with the round's
+// fields in record slots 5, 6 (near parts included); returns, in every lane,
+// whether a float32 sum (MIX) was ill-conditioned (kappa test).
+constexpr int kWarpRuns = kWarpChunk / SPT_BLOCK_SEGS;
+static_assert(kWarpRuns <= 32, "one lane classifies each run of a chunk");
 
 template <int NP, int NQ, bool MIX>
-__device__ void far_adaptive(Ctx& c, int r0, int np_, unsigned long long& far_evals) {
+__device__ bool far_adaptive_warp(Ctx& c, int r0, int np_, unsigned long long& far_evals) {
     const SptBem& b = c.bem;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nseg = b.n_seg, nps = b.nodes_per_seg;
     double* P = c.bpt;
-    int* lists = reinterpret_cast<int*>(c.tiles);  // L0 | L1 | L2, kAdaptSegs each
-    unsigned char* mask = c.nflag;                 // near masks of L0
-    // counts and run lists in the reduction scratch (free until the final reduction)
-    int* s_wc = reinterpret_cast<int*>(c.red);     // [3][kMaxWarps] per-warp level counts
-    int* s_n = s_wc + 24;                          // [3] lengths of L0, L1, L2
-    int* s_rn = s_wc + 27;                         // [3] lengths of R2, R3, M
-    int* R2 = s_wc + 32;
-    int* R3 = s_wc + 64;
-    int* M = s_wc + 96;
-    int* Mcls = s_wc + 128;
+    int* scratch = reinterpret_cast<int*>(c.tiles) + warp * kWarpScratchInts;
+    int* lists = scratch;                                                    // L0 | L1 | L2, kWarpChunk each
+    unsigned char* mask = reinterpret_cast<unsigned char*>(scratch + 3 * kWarpChunk);  // near masks of L0
+    int* R2 = scratch + 3 * kWarpChunk + kWarpChunk / 4;
+    int* R3 = R2 + kWarpRuns;
+    int* M = R3 + kWarpRuns;
+    int* Mcls = M + kWarpRuns;
     double pr[NP], pinv[NP], pz[NP], ar[NP], az[NP];
     float fr[NP], fz[NP], kr[NP], kz[NP], prf[NP], pinvf[NP];
     float sa[NP];
@@ -606,120 +611,108 @@ __device__ void far_adaptive(Ctx& c, int r0, int np_, unsigned long long& far_ev
         prf[p] = (float)pr[p];
         pinvf[p] = (float)pinv[p];
     }
-    if (MIX && tid == 0) *c.redo = 0;  // ordered before the reduction's writes by the barriers between
     const double r4 = b.ratio4, r2 = b.ratio2;
     const double* cr = b.coarse;
     const double* cz = b.coarse + b.coarse_stride;
     const double* cw = b.coarse + 2 * b.coarse_stride;
     const bool run_rule = b.blk && b.run_nodes && b.ratio_run > 0.0;
     const unsigned lt = (1u << lane) - 1u;
-    for (int c0 = 0; c0 < nseg; c0 += kAdaptSegs) {
+    for (int c0 = 0; c0 < nseg; c0 += kWarpChunk) {
         const int q0 = c0 / SPT_BLOCK_SEGS;
-        const int nr = min(kAdaptRuns, (nseg - c0 + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS);
-        if (warp == 0) {
-            const int q = q0 + lane;
-            int cls = -1;  // 3 run rule, 2 Gauss-2 on every segment, 1 no near segment, 0 full test
-            if (lane < nr) {
-                cls = 0;
-                if (b.blk) {
-                    double lb = INFINITY;
-                    for (int p = 0; p < np_; ++p) lb = fmin(lb, blk_lower(b, q, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4]));
-                    const double lm = blk_lmax(b, q);
-                    if (run_rule && __ldg(b.blk + 5 * b.blk_stride + q) != 0.0 &&
-                        lb >= b.ratio_run * __ldg(b.blk + 4 * b.blk_stride + q))
-                        cls = 3;
-                    else if (lb >= r2 * lm) cls = 2;
-                    else if (lb >= r4 * lm) cls = 1;
-                }
+        const int nr = min(kWarpRuns, (nseg - c0 + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS);
+        const int q = q0 + lane;
+        int cls = -1;  // 3 run rule, 2 Gauss-2 on every segment, 1 no near segment, 0 full test
+        if (lane < nr) {
+            cls = 0;
+            if (b.blk) {
+                double lb = INFINITY;
+                for (int p = 0; p < np_; ++p) lb = fmin(lb, blk_lower(b, q, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4]));
+                const double lm = blk_lmax(b, q);
+                if (run_rule && __ldg(b.blk + 5 * b.blk_stride + q) != 0.0 &&
+                    lb >= b.ratio_run * __ldg(b.blk + 4 * b.blk_stride + q))
+                    cls = 3;
+                else if (lb >= r2 * lm) cls = 2;
+                else if (lb >= r4 * lm) cls = 1;
             }
-            const unsigned b3 = __ballot_sync(0xffffffffu, cls == 3);
-            const unsigned b2 = __ballot_sync(0xffffffffu, cls == 2);
-            const unsigned bm = __ballot_sync(0xffffffffu, cls == 0 || cls == 1);
-            if (cls == 3) R3[__popc(b3 & lt)] = q;
-            if (cls == 2) R2[__popc(b2 & lt)] = q;
-            if (cls == 0 || cls == 1) { M[__popc(bm & lt)] = q; Mcls[__popc(bm & lt)] = cls; }
-            if (lane == 0) { s_rn[0] = __popc(b2); s_rn[1] = __popc(b3); s_rn[2] = __popc(bm); }
-            if (lane < 3) s_n[lane] = 0;
         }
-        __syncthreads();
-        // segment classification of the M runs: one run per warp per wave
-        const int nm = s_rn[2];
-        for (int w0 = 0; w0 < nm; w0 += c.nw) {
-            const int mi = w0 + warp;
+        const unsigned b3 = __ballot_sync(0xffffffffu, cls == 3);
+        const unsigned b2 = __ballot_sync(0xffffffffu, cls == 2);
+        const unsigned bm = __ballot_sync(0xffffffffu, cls == 0 || cls == 1);
+        if (cls == 3) R3[__popc(b3 & lt)] = q;
+        if (cls == 2) R2[__popc(b2 & lt)] = q;
+        if (cls == 0 || cls == 1) { M[__popc(bm & lt)] = q; Mcls[__popc(bm & lt)] = cls; }
+        const int nR2 = __popc(b2), nR3 = __popc(b3), nm = __popc(bm);
+        __syncwarp();
+        // segment classification of the M runs, one run at a time (lane = segment)
+        int n0 = 0, n1 = 0, n2 = 0;
+        for (int mi = 0; mi < nm; ++mi) {
+            const int sg = M[mi] * SPT_BLOCK_SEGS + lane;
             int lvl = 3;
             unsigned m = 0;
-            int sg = 0;
-            if (mi < nm) {
-                sg = M[mi] * SPT_BLOCK_SEGS + lane;
-                if (sg < nseg) {
-                    const int cls = Mcls[mi];
-                    const double L = segf(b, 4, sg);
-                    double dmin = INFINITY;
-                    for (int p = 0; p < np_; ++p) {
-                        double proj, dist;
-                        if (seg_near(b, sg, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4], proj, dist)) m |= 1u << p;
-                        dmin = fmin(dmin, dist);
-                    }
-                    if (cls == 1) m = 0, lvl = dmin < r2 * L ? 1 : 2;
-                    else lvl = dmin < r4 * L ? 0 : (dmin < r2 * L ? 1 : 2);
+            if (sg < nseg) {
+                const int mc = Mcls[mi];
+                const double L = segf(b, 4, sg);
+                double dmin = INFINITY;
+                for (int p = 0; p < np_; ++p) {
+                    double proj, dist;
+                    if (seg_near(b, sg, P[8 * (r0 + p) + 3], P[8 * (r0 + p) + 4], proj, dist)) m |= 1u << p;
+                    dmin = fmin(dmin, dist);
                 }
+                if (mc == 1) m = 0, lvl = dmin < r2 * L ? 1 : 2;
+                else lvl = dmin < r4 * L ? 0 : (dmin < r2 * L ? 1 : 2);
             }
-            unsigned bal[3];
-#pragma unroll
-            for (int v = 0; v < 3; ++v) {
-                bal[v] = __ballot_sync(0xffffffffu, lvl == v);
-                if (lane == 0) s_wc[v * kMaxWarps + warp] = __popc(bal[v]);
+            const unsigned v0 = __ballot_sync(0xffffffffu, lvl == 0);
+            const unsigned v1 = __ballot_sync(0xffffffffu, lvl == 1);
+            const unsigned v2 = __ballot_sync(0xffffffffu, lvl == 2);
+            if (lvl == 0) {
+                const int pos = n0 + __popc(v0 & lt);
+                lists[pos] = sg;
+                mask[pos] = (unsigned char)m;
+            } else if (lvl == 1) {
+                lists[kWarpChunk + n1 + __popc(v1 & lt)] = sg;
+            } else if (lvl == 2) {
+                lists[2 * kWarpChunk + n2 + __popc(v2 & lt)] = sg;
             }
-            __syncthreads();
-            if (lvl < 3) {
-                int pos = s_n[lvl] + __popc(bal[lvl] & lt);
-                for (int w = 0; w < warp; ++w) pos += s_wc[lvl * kMaxWarps + w];
-                lists[lvl * kAdaptSegs + pos] = sg;
-                if (lvl == 0) mask[pos] = (unsigned char)m;
-            }
-            __syncthreads();
-            if (tid < 3) {
-                int t = 0;
-                for (int w = 0; w < c.nw; ++w) t += s_wc[tid * kMaxWarps + w];
-                s_n[tid] += t;
-            }
-            __syncthreads();
+            n0 += __popc(v0);
+            n1 += __popc(v1);
+            n2 += __popc(v2);
         }
-        const int e0 = s_n[0] * nps, e1 = e0 + 4 * s_n[1], e2 = e1 + 2 * s_n[2];
-        const int e3 = e2 + 2 * SPT_BLOCK_SEGS * s_rn[0], e4 = e3 + SPT_RUN_NODES * s_rn[1];
-        for (int q0i = tid; q0i < e4; q0i += c.nt * NQ) {
+        __syncwarp();
+        const int e0 = n0 * nps, e1 = e0 + 4 * n1, e2 = e1 + 2 * n2;
+        const int e3 = e2 + 2 * SPT_BLOCK_SEGS * nR2, e4 = e3 + SPT_RUN_NODES * nR3;
+        for (int q0i = lane; q0i < e4; q0i += 32 * NQ) {
             double rq[NQ], zq[NQ], wq[NQ];
             unsigned mk[NQ];
             bool in[NQ];
 #pragma unroll
             for (int j = 0; j < NQ; ++j) {
-                const int q = q0i + j * c.nt;
-                in[j] = q < e4;
+                const int qq = q0i + j * 32;
+                in[j] = qq < e4;
                 size_t src = 0;
                 const double *tr = cr, *tz = cz, *tw = cw;
                 mk[j] = 0;
                 if (!in[j]) {
                     // padding lane: any valid node, not accumulated
-                } else if (q < e0) {
-                    const int li = q / nps;
-                    src = (size_t)lists[li] * nps + (q - li * nps);
+                } else if (qq < e0) {
+                    const int li = qq / nps;
+                    src = (size_t)lists[li] * nps + (qq - li * nps);
                     tr = b.node;
                     tz = b.node + b.node_stride;
                     tw = b.node + 2 * b.node_stride;
                     mk[j] = mask[li];
-                } else if (q < e1) {
-                    const int i = q - e0;
-                    src = (size_t)lists[kAdaptSegs + (i >> 2)] * 6 + (i & 3);
-                } else if (q < e2) {
-                    const int i = q - e1;
-                    src = (size_t)lists[2 * kAdaptSegs + (i >> 1)] * 6 + 4 + (i & 1);
-                } else if (q < e3) {
-                    const int i = q - e2;
+                } else if (qq < e1) {
+                    const int i = qq - e0;
+                    src = (size_t)lists[kWarpChunk + (i >> 2)] * 6 + (i & 3);
+                } else if (qq < e2) {
+                    const int i = qq - e1;
+                    src = (size_t)lists[2 * kWarpChunk + (i >> 1)] * 6 + 4 + (i & 1);
+                } else if (qq < e3) {
+                    const int i = qq - e2;
                     const int sgi = R2[i / (2 * SPT_BLOCK_SEGS)] * SPT_BLOCK_SEGS + ((i & (2 * SPT_BLOCK_SEGS - 1)) >> 1);
                     if (sgi < nseg) src = (size_t)sgi * 6 + 4 + (i & 1);
                     else in[j] = false;  // past the last segment of a short final run
                 } else {
-                    const int i = q - e3;
+                    const int i = qq - e3;
                     src = (size_t)R3[i / SPT_RUN_NODES] * SPT_RUN_NODES + (i % SPT_RUN_NODES);
                     tr = b.run_nodes;
                     tz = b.run_nodes + b.run_stride;
@@ -763,9 +756,31 @@ __device__ void far_adaptive(Ctx& c, int r0, int np_, unsigned long long& far_ev
                 }
             }
         }
-        __syncthreads();  // the lists are rewritten by the next chunk
+        __syncwarp();  // the lists are rewritten by the next chunk
     }
-    round_reduce<NP, MIX>(c, r0, np_, ar, az, fr, fz, kr, kz, sa);
+    // fixed-order warp reduction; lane 0 writes the round's fields
+    bool redo = false;
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+        if (MIX) {
+            ar[p] += (double)fr[p] - (double)kr[p];
+            az[p] += (double)fz[p] - (double)kz[p];
+        }
+        const double vr = warp_sum(ar[p]);
+        const double vz = warp_sum(az[p]);
+        const double va = MIX ? warp_sum((double)sa[p]) : 0.0;
+        if (lane == 0 && p < np_) {
+            const int k = r0 + p;
+            const double er = vr + P[8 * k + 7], ez = vz + c.fld[3 * k + 2];
+            P[8 * k + 5] = er;
+            P[8 * k + 6] = ez;
+            if (MIX) {
+                const double tz = ez + c.g.E_gun;
+                if (!(va <= c.kappa * sqrt(er * er + tz * tz))) redo = true;
+            }
+        }
+    }
+    return __shfl_sync(0xffffffffu, redo, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -857,21 +872,32 @@ static __device__ void bem_closest(Ctx& c, int n, bool frame) {
 }
 
 
-// One far-sum round of the far rule FAR: the NP x NQ tile shape of far_round
-// or far_adaptive.
-template <int NP, int NQ, bool MIX, int FAR>
-__device__ __forceinline__ void far_pass(Ctx& c, int r0, int np_, int n_tiles, int segs_per_tile, bool& ok,
-                                         unsigned long long& fe) {
-    if constexpr (FAR == SPT_FAR_ADAPTIVE)
-        far_adaptive<NP, NQ, MIX>(c, r0, np_, fe);
-    else
-        far_round<NP, NQ, MIX>(c, r0, np_, n_tiles, segs_per_tile, ok, fe);
+// Adaptive far rule: one round of np_ points by this warp, float32 first in
+// the mixed form, float64 again when that round is ill-conditioned.  The
+// float64 tile shapes are the float64 form's, so with every round redone the
+// mixed form reproduces it bit for bit.
+template <int FORM>
+__device__ __forceinline__ void warp_round(Ctx& c, int r0, int np_, unsigned long long& fe) {
+    if constexpr (FORM == SPT_FORM_FP64) {
+        if (np_ == 1) far_adaptive_warp<1, 8, false>(c, r0, np_, fe);
+        else if (np_ == 2) far_adaptive_warp<2, 4, false>(c, r0, np_, fe);
+        else far_adaptive_warp<4, 2, false>(c, r0, np_, fe);
+    } else {
+        // float32 tiles keep 4 ring evaluations in flight per lane (8 spill at
+        // 128 registers; more resident warps supply the parallelism instead)
+        bool redo;
+        if (np_ == 1) redo = far_adaptive_warp<1, 4, true>(c, r0, np_, fe);
+        else if (np_ == 2) redo = far_adaptive_warp<2, 2, true>(c, r0, np_, fe);
+        else redo = far_adaptive_warp<4, 1, true>(c, r0, np_, fe);
+        if (redo) {
+            if ((threadIdx.x & 31) == 0) atomicAdd(c.cnt + SPT_CNT_FP64_ROUNDS, 1ull);
+            if (np_ == 1) far_adaptive_warp<1, 8, false>(c, r0, np_, fe);
+            else if (np_ == 2) far_adaptive_warp<2, 4, false>(c, r0, np_, fe);
+            else far_adaptive_warp<4, 2, false>(c, r0, np_, fe);
+        }
+    }
 }
 
-// B + C: exact BEM field (E_rho, E_z into record slots 5, 6) of records [0, n)
-// whose slots 3, 4 hold the evaluation point.  FORM: SPT_FORM_FP64 sums in
-// float64; the other forms sum in float32 first and redo an ill-conditioned
-// round in float64.
 template <int FORM, int FAR>
 __device__ __forceinline__ void bem_sums(Ctx& c, int n, int* status_flag) {
     const SptBem& b = c.bem;
@@ -938,37 +964,47 @@ __device__ __forceinline__ void bem_sums(Ctx& c, int n, int* status_flag) {
     count_add(c, SPT_CNT_RING_NEAR, n_ring_near);
     __syncthreads();
 
-    // C: far sum, rounds of up to c.round_pts points over TMA-staged node tiles;
-    // the round's point count selects how many nodes each thread keeps in
-    // flight so that every thread has 8 independent ring evaluations.
-    const int tile_cap = c.L.tile_cap;
-    const int segs_per_tile = min(tile_cap / nps, 256);
-    const int n_tiles = (nseg + segs_per_tile - 1) / segs_per_tile;
+    // C: far sum.  Adaptive rule: rounds of up to c.round_pts points, each
+    // owned by one warp (as many rounds as warps where the points allow, so
+    // no warp waits for another until the end).  Reference rule: rounds over
+    // TMA-staged node tiles shared by the whole CTA; the round's point count
+    // selects how many nodes each thread keeps in flight.
     unsigned long long far_evals = 0;
     bool ok = true;
-    for (int r0 = 0; r0 < n; r0 += c.round_pts) {
-        const int np_ = min(c.round_pts, n - r0);
-        // mixed form (and the exact sums of the learned form): float32 first,
-        // float64 again for a round whose float32 sums are ill-conditioned
-        if constexpr (FORM == SPT_FORM_FP64) {
-            if (np_ == 1) far_pass<1, 8, false, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            else if (np_ == 2) far_pass<2, 4, false, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            else far_pass<4, 2, false, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-        } else {
-            // float32 tiles keep 4 ring evaluations in flight per thread (8 spill
-            // at 128 registers; the narrower CTAs supply the parallelism instead)
-            if (np_ == 1) far_pass<1, 4, true, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            else if (np_ == 2) far_pass<2, 2, true, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            else far_pass<4, 1, true, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-            const bool redo = *c.redo != 0;
-            // every thread has read the flag before the next round's float32 pass resets it
-            __syncthreads();
-            if (redo) {
-                if (tid == 0) atomicAdd(c.cnt + SPT_CNT_FP64_ROUNDS, 1ull);
-                // the tile shape the float64 form takes for this round size (same sums, bit for bit)
-                if (np_ == 1) far_pass<1, 8, false, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-                else if (np_ == 2) far_pass<2, 4, false, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
-                else far_pass<4, 2, false, FAR>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+    if constexpr (FAR == SPT_FAR_ADAPTIVE) {
+        const int per = min(c.round_pts, max(1, (n + c.nw - 1) / c.nw));
+        const int n_rounds = (n + per - 1) / per;
+        for (int r = warp; r < n_rounds; r += c.nw) {
+            const int r0 = r * per;
+            warp_round<FORM>(c, r0, min(per, n - r0), far_evals);
+        }
+        __syncthreads();
+    } else {
+        const int tile_cap = c.L.tile_cap;
+        const int segs_per_tile = min(tile_cap / nps, 256);
+        const int n_tiles = (nseg + segs_per_tile - 1) / segs_per_tile;
+        for (int r0 = 0; r0 < n; r0 += c.round_pts) {
+            const int np_ = min(c.round_pts, n - r0);
+            if constexpr (FORM == SPT_FORM_FP64) {
+                if (np_ == 1) far_round<1, 8, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                else if (np_ == 2) far_round<2, 4, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                else far_round<4, 2, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+            } else {
+                // mixed form (and the exact sums of the learned form): float32 first,
+                // float64 again for a round whose float32 sums are ill-conditioned
+                if (np_ == 1) far_round<1, 4, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                else if (np_ == 2) far_round<2, 2, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                else far_round<4, 1, true>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                const bool redo = *c.redo != 0;
+                // every thread has read the flag before the next round's float32 pass resets it
+                __syncthreads();
+                if (redo) {
+                    if (tid == 0) atomicAdd(c.cnt + SPT_CNT_FP64_ROUNDS, 1ull);
+                    // the tile shape the float64 form takes for this round size (same sums, bit for bit)
+                    if (np_ == 1) far_round<1, 8, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                    else if (np_ == 2) far_round<2, 4, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                    else far_round<4, 2, false>(c, r0, np_, n_tiles, segs_per_tile, ok, far_evals);
+                }
             }
         }
     }
@@ -2009,7 +2045,7 @@ struct TraceLaunch {
 template <int KIND, int FORM, int FAR>
 int trace_grid(int max_group_size, int threads, int n_groups, long long max_slots, size_t* smem, int* grid,
                int* per_sm) {
-    const Layout L = make_layout(max_group_size, FAR, FORM == SPT_FORM_SURROGATE);
+    const Layout L = make_layout(max_group_size, FAR, FORM == SPT_FORM_SURROGATE, true, threads / 32);
     auto kern = trace_kernel<KIND, FORM, FAR>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
     if (e != cudaSuccess) return (int)e;
