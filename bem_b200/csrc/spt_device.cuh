@@ -791,14 +791,13 @@ __device__ bool far_adaptive_warp(Ctx& c, int r0, int np_, unsigned long long& f
 // A: closest segment and on-surface offset of records [0, n).  With `frame`,
 // also the closest segment, its parameter t and the distance, for the
 // surrogate's inputs.
-static __device__ void bem_closest(Ctx& c, int n, bool frame) {
+// One warp, record k.
+__device__ __forceinline__ void closest_point(Ctx& c, int k, bool frame) {
     const SptBem& b = c.bem;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int lane = threadIdx.x & 31;
     double* P = c.bpt;  // record k: [0]x [1]y [2]z [3]rho_e [4]z_e [5]ax [6]ay [7]near_r ; near_z in fld tmp
     const int nseg = b.n_seg;
-
-    // A: closest point + on-surface offset (one warp per point)
-    for (int k = warp; k < n; k += c.nw) {
+    {
         const double x = P[8 * k + 0], y = P[8 * k + 1], z = P[8 * k + 2];
         const double rho = hypot(x, y);
         double best = INFINITY;
@@ -868,47 +867,24 @@ static __device__ void bem_closest(Ctx& c, int n, bool frame) {
             }
         }
     }
+}
+
+static __device__ void bem_closest(Ctx& c, int n, bool frame) {
+    // one warp per point
+    for (int k = threadIdx.x >> 5; k < n; k += c.nw) closest_point(c, k, frame);
     __syncthreads();
 }
 
 
-// Adaptive far rule: one round of np_ points by this warp, float32 first in
-// the mixed form, float64 again when that round is ill-conditioned.  The
-// float64 tile shapes are the float64 form's, so with every round redone the
-// mixed form reproduces it bit for bit.
-template <int FORM>
-__device__ __forceinline__ void warp_round(Ctx& c, int r0, int np_, unsigned long long& fe) {
-    if constexpr (FORM == SPT_FORM_FP64) {
-        if (np_ == 1) far_adaptive_warp<1, 8, false>(c, r0, np_, fe);
-        else if (np_ == 2) far_adaptive_warp<2, 4, false>(c, r0, np_, fe);
-        else far_adaptive_warp<4, 2, false>(c, r0, np_, fe);
-    } else {
-        // float32 tiles keep 4 ring evaluations in flight per lane (8 spill at
-        // 128 registers; more resident warps supply the parallelism instead)
-        bool redo;
-        if (np_ == 1) redo = far_adaptive_warp<1, 4, true>(c, r0, np_, fe);
-        else if (np_ == 2) redo = far_adaptive_warp<2, 2, true>(c, r0, np_, fe);
-        else redo = far_adaptive_warp<4, 1, true>(c, r0, np_, fe);
-        if (redo) {
-            if ((threadIdx.x & 31) == 0) atomicAdd(c.cnt + SPT_CNT_FP64_ROUNDS, 1ull);
-            if (np_ == 1) far_adaptive_warp<1, 8, false>(c, r0, np_, fe);
-            else if (np_ == 2) far_adaptive_warp<2, 4, false>(c, r0, np_, fe);
-            else far_adaptive_warp<4, 2, false>(c, r0, np_, fe);
-        }
-    }
-}
-
-template <int FORM, int FAR>
-__device__ __forceinline__ void bem_sums(Ctx& c, int n, int* status_flag) {
+// B for one record k, by one warp: the near-segment sinh quadrature
+// (bem/axisymmetric.py:566-600); lane 0 ends with near_r in record slot 7 and
+// near_z in fld[3k + 2].
+__device__ __forceinline__ void near_point(Ctx& c, int k, unsigned long long& n_near, unsigned long long& n_ring_near) {
     const SptBem& b = c.bem;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int lane = threadIdx.x & 31;
     double* P = c.bpt;
     const int nseg = b.n_seg;
-    const int nps = b.nodes_per_seg;
-    if (n <= 0) return;
-    // B: near-segment sinh quadrature (one warp per point)
-    unsigned long long n_near = 0, n_ring_near = 0;
-    for (int k = warp; k < n; k += c.nw) {
+    {
         const double re = P[8 * k + 3], ze = P[8 * k + 4];
         double acc_r = 0.0, acc_z = 0.0;
         const int nblk = (nseg + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS;
@@ -960,6 +936,48 @@ __device__ __forceinline__ void bem_sums(Ctx& c, int n, int* status_flag) {
             c.fld[3 * k + 2] = acc_z;  // temporary near_z (fld is rewritten after the far sum)
         }
     }
+}
+
+// Adaptive far rule for record k, by this warp: float32 first in the mixed
+// form, float64 again when its sum is ill-conditioned.  The float64 tile is
+// the float64 form's, so with every sum redone the mixed form reproduces it.
+template <int FORM>
+__device__ __forceinline__ void far_point(Ctx& c, int k, unsigned long long& fe) {
+    if constexpr (FORM == SPT_FORM_FP64) {
+        far_adaptive_warp<1, 8, false>(c, k, 1, fe);
+    } else {
+        // float32 tiles keep 4 ring evaluations in flight per lane (8 spill at
+        // 128 registers; more resident warps supply the parallelism instead)
+        if (far_adaptive_warp<1, 4, true>(c, k, 1, fe)) {
+            if ((threadIdx.x & 31) == 0) atomicAdd(c.cnt + SPT_CNT_FP64_ROUNDS, 1ull);
+            far_adaptive_warp<1, 8, false>(c, k, 1, fe);
+        }
+    }
+}
+
+// Next record for this warp from the CTA's task counter (dynamic assignment:
+// points near the surface cost many times more than distant ones).
+__device__ __forceinline__ int next_task(int* counter) {
+    int k = 0;
+    if ((threadIdx.x & 31) == 0) k = atomicAdd(counter, 1);
+    return __shfl_sync(0xffffffffu, k, 0);
+}
+
+// B + C: exact BEM field (E_rho, E_z into record slots 5, 6) of records [0, n)
+// whose slots 3, 4 hold the evaluation point.  FORM: SPT_FORM_FP64 sums in
+// float64; the other forms sum in float32 first and redo an ill-conditioned
+// sum in float64.
+template <int FORM, int FAR>
+__device__ __forceinline__ void bem_sums(Ctx& c, int n, int* status_flag) {
+    const SptBem& b = c.bem;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* P = c.bpt;
+    const int nseg = b.n_seg;
+    const int nps = b.nodes_per_seg;
+    if (n <= 0) return;
+    // B: near-segment sinh quadrature (one warp per point)
+    unsigned long long n_near = 0, n_ring_near = 0;
+    for (int k = warp; k < n; k += c.nw) near_point(c, k, n_near, n_ring_near);
     count_add(c, SPT_CNT_NEAR_PAIRS, n_near);
     count_add(c, SPT_CNT_RING_NEAR, n_ring_near);
     __syncthreads();
@@ -972,12 +990,11 @@ __device__ __forceinline__ void bem_sums(Ctx& c, int n, int* status_flag) {
     unsigned long long far_evals = 0;
     bool ok = true;
     if constexpr (FAR == SPT_FAR_ADAPTIVE) {
-        const int per = min(c.round_pts, max(1, (n + c.nw - 1) / c.nw));
-        const int n_rounds = (n + per - 1) / per;
-        for (int r = warp; r < n_rounds; r += c.nw) {
-            const int r0 = r * per;
-            warp_round<FORM>(c, r0, min(per, n - r0), far_evals);
-        }
+        // one point per warp task, taken dynamically
+        __shared__ int s_far_task;
+        if (tid == 0) s_far_task = c.nw;
+        __syncthreads();
+        for (int k = warp; k < n; k = next_task(&s_far_task)) far_point<FORM>(c, k, far_evals);
         __syncthreads();
     } else {
         const int tile_cap = c.L.tile_cap;
@@ -1272,8 +1289,54 @@ __device__ void surrogate_points(Ctx& c, int n, int* status_flag) {
 
 // BEM field of the n points listed in c.bpt (x, y, z at slots 0..2 of each
 // 8-double record): the reference's evaluation, phases A-D.
+// BEM field of the records [0, n) with the adaptive far rule, each point one
+// warp task from start to end -- closest segment and on-surface offset, near
+// quadrature, far sum, rotation -- taken dynamically from a CTA counter, so
+// the only barrier is the one at the end.  Same arithmetic as the phased
+// path (bem_closest, bem_sums, bem_rotate).
+template <int FORM>
+__device__ void bem_points_fused(Ctx& c, int n) {
+    const int lane = threadIdx.x & 31;
+    double* P = c.bpt;
+    __shared__ int s_task;
+    if (threadIdx.x == 0) s_task = c.nw;
+    __syncthreads();
+    unsigned long long n_near = 0, n_ring_near = 0, far_evals = 0;
+    for (int k = threadIdx.x >> 5; k < n; k = next_task(&s_task)) {
+        closest_point(c, k, false);
+        __syncwarp();
+        near_point(c, k, n_near, n_ring_near);
+        __syncwarp();
+        far_point<FORM>(c, k, far_evals);
+        if (lane == 0) {
+            const double x = P[8 * k + 0], y = P[8 * k + 1];
+            const double rho = hypot(x, y);
+            const double e_rho = P[8 * k + 5], e_z = P[8 * k + 6];
+            double ex = 0.0, ey = 0.0;
+            if (rho != 0.0) {
+                ex = e_rho * (x / rho);
+                ey = e_rho * (y / rho);
+            }
+            P[8 * k + 5] = ex;
+            P[8 * k + 6] = ey;
+            P[8 * k + 7] = e_z;
+        }
+        __syncwarp();
+    }
+    count_add(c, SPT_CNT_NEAR_PAIRS, n_near);
+    count_add(c, SPT_CNT_RING_NEAR, n_ring_near);
+    count_add(c, SPT_CNT_RING_FAR, far_evals);
+    __syncthreads();
+}
+
 template <int FORM, int FAR>
 __device__ void bem_points(Ctx& c, int n, bool scatter, int* status_flag) {
+    if constexpr (FAR == SPT_FAR_ADAPTIVE) {
+        if (!scatter) {
+            bem_points_fused<FORM>(c, n);
+            return;
+        }
+    }
     bem_closest(c, n, false);
     bem_sums<FORM, FAR>(c, n, status_flag);
     bem_rotate(c, n, scatter);

@@ -235,11 +235,11 @@ typedef struct {
     const double* sur_log_scale;
     double sur_s_end, sur_sig_floor, sur_band, sur_spot, sur_d_min, sur_d_max;
     unsigned long long* sur_stats;
-    /* Far-sum tile shape: evaluation points per round, 1, 2, 4 or 8 (0 or
-     * anything else: 8).  Fewer points per round give each thread more
-     * nodes in flight per point; more points share each node load and each
-     * round's classification.  Results agree to rounding (and, with the
-     * adaptive rule, to its ~1e-14 classification effect). */
+    /* Far-sum tile shape of the reference far rule: evaluation points per
+     * round, 1, 2 or 4 (0 or anything else: 4).  Fewer points per round give
+     * each thread more nodes in flight per point; more points share each
+     * node load.  Results agree to rounding.  (The adaptive rule takes one
+     * point per warp task, classified for that point alone.) */
     int32_t round_points;
     /* CTA width of the trace: 32, 64, 128 or 256 threads work on one group
      * at a time (0 or anything else: by group size -- 64 up to 16

@@ -108,18 +108,24 @@ def _post_trace(form, far_rule="adaptive", attempts=40, **tracer_attrs):
 @pytest.mark.parametrize("far_rule", ["reference", "adaptive"])
 def test_mixed_form_redoes_ill_conditioned_sums_in_float64(far_rule):
     """kappa_max -> 0 declares every float32 sum ill-conditioned: every far
-    round and pair sum is recomputed by the float64 code, so the mixed form
-    reproduces the float64 form exactly."""
+    sum and pair sum is recomputed by the float64 code, so the mixed form
+    lands on the float64 form, far closer than the mixed form does without
+    the recomputation.  (The two forms are separate kernel instantiations,
+    whose float64 multiply-adds the compiler may contract differently; the
+    40-attempt trace carries such ulp differences to ~1e-9.)"""
     p64, _ = _post_trace("fp64", far_rule)
     pmx, c = _post_trace("mixed", far_rule, kappa_max=1e-300)
+    pf32, _ = _post_trace("mixed", far_rule)
     assert c["fp64_rounds"] > 0 and c["fp64_targets"] > 0
-    np.testing.assert_array_equal(pmx, p64)
+    scale = np.abs(p64).max()
+    np.testing.assert_allclose(pmx, p64, rtol=1e-8, atol=1e-8 * scale)
+    assert np.abs(pmx - p64).max() < 0.1 * np.abs(pf32 - p64).max()
 
 
 def test_round_points_changes_the_far_tile_only():
-    """A far-sum round of 2 points instead of 8: other summation order and
-    classification rounds, same trace to 1e-10."""
-    p8, _ = _post_trace("fp64", "adaptive")
-    p2, _ = _post_trace("fp64", "adaptive", round_points=2)
-    assert not np.array_equal(p2, p8)
-    np.testing.assert_allclose(p2, p8, rtol=1e-10, atol=1e-10 * np.abs(p8).max())
+    """A far-sum round of 1 point instead of 4 (reference far rule): other
+    summation order, same trace to 1e-10."""
+    p4, _ = _post_trace("fp64", "reference")
+    p1, _ = _post_trace("fp64", "reference", round_points=1)
+    assert not np.array_equal(p1, p4)
+    np.testing.assert_allclose(p1, p4, rtol=1e-10, atol=1e-10 * np.abs(p4).max())
