@@ -203,7 +203,7 @@ def _adaptive_override(er_s, ez_s, rho_e, z_e, dist, seg, coarse, ratio4, ratio2
 
 
 def field(points, profile, sigma, n_subdiv=8, chunk=256, far_rule="reference", ratio4=8.0, ratio2=300.0,
-          round_size=8, run_flags=None, ratio_run=4.0):
+          round_size=1, run_flags=None, ratio_run=4.0):
     """bem/axisymmetric.py:501-605 -- E = -grad S[sigma] at points (..., 3).
 
     far_rule="adaptive" swaps the sub-panel sums of distant segments for the
