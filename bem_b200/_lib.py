@@ -18,7 +18,7 @@ FAR_REFERENCE, FAR_ADAPTIVE = 0, 1
 FAR_RULES = {"reference": FAR_REFERENCE, "adaptive": FAR_ADAPTIVE}
 GROUP_NEW, GROUP_RUNNING, GROUP_DONE, GROUP_NONFINITE, GROUP_TIMEOUT = 0, 1, 2, 3, 4
 COUNTERS = ("attempts", "accepted", "particle_steps", "stage_evals", "pair_evals", "ring_far", "ring_near",
-            "near_pairs", "fp64_rounds", "fp64_targets", "live_steps")
+            "near_pairs", "fp64_rounds", "fp64_targets", "live_steps", "cluster_evals")
 N_COUNTERS = len(COUNTERS)
 SEG_FIELDS = 11
 BLOCK_SEGS = 32
@@ -41,7 +41,8 @@ class SptBem(ctypes.Structure):
                 ("seg", _p), ("node", _p), ("gauss8_x", _d * 8), ("gauss8_w", _d * 8),
                 ("far_rule", _i32), ("reserved", _i32), ("ratio4", _d), ("ratio2", _d), ("coarse", _p),
                 ("coarse_stride", _i64), ("blk", _p), ("blk_stride", _i64), ("ratio_run", _d), ("run_nodes", _p),
-                ("run_stride", _i64)]
+                ("run_stride", _i64), ("clusters", _p), ("cluster_levels", _i32), ("cluster_terms", _i32),
+                ("cluster_kappa", _d)]
 
 
 class SptState(ctypes.Structure):

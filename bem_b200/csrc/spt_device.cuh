@@ -188,7 +188,8 @@ struct Layout {
 // kWarpScratchInts ints: three segment lists of kWarpChunk entries, the
 // near masks of the first (kWarpChunk bytes) and four run lists.
 constexpr int kWarpChunk = 256;
-constexpr int kWarpScratchInts = 3 * kWarpChunk + kWarpChunk / 4 + 4 * (kWarpChunk / SPT_BLOCK_SEGS);
+constexpr int kWarpScratchInts = 3 * kWarpChunk + kWarpChunk / 4 + 4 * (kWarpChunk / SPT_BLOCK_SEGS) +
+                                  SPT_MAX_CLUSTER_RUNS / 32;
 static_assert(kWarpScratchInts % 2 == 0, "per-warp scratch keeps 8-byte alignment");
 
 // Shared-memory layout of one CTA for groups of up to E particles.  The far
@@ -580,11 +581,67 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
 // Without run bounds every run is in M.  Lane 0 ends with the round's
 // fields in record slots 5, 6 (near parts included); returns, in every lane,
 // whether a float32 sum (MIX) was ill-conditioned (kappa test).
+// Recurrence constants of the Legendre polynomials, P_(n+1) = a_n u P_n - b_n P_(n-1).
+static __device__ __constant__ double kLegA[64] = {
+#define SPT_LA(n) (2.0 * (n) + 1.0) / ((n) + 1.0)
+    SPT_LA(0), SPT_LA(1), SPT_LA(2), SPT_LA(3), SPT_LA(4), SPT_LA(5), SPT_LA(6), SPT_LA(7), SPT_LA(8), SPT_LA(9),
+    SPT_LA(10), SPT_LA(11), SPT_LA(12), SPT_LA(13), SPT_LA(14), SPT_LA(15), SPT_LA(16), SPT_LA(17), SPT_LA(18),
+    SPT_LA(19), SPT_LA(20), SPT_LA(21), SPT_LA(22), SPT_LA(23), SPT_LA(24), SPT_LA(25), SPT_LA(26), SPT_LA(27),
+    SPT_LA(28), SPT_LA(29), SPT_LA(30), SPT_LA(31), SPT_LA(32), SPT_LA(33), SPT_LA(34), SPT_LA(35), SPT_LA(36),
+    SPT_LA(37), SPT_LA(38), SPT_LA(39), SPT_LA(40), SPT_LA(41), SPT_LA(42), SPT_LA(43), SPT_LA(44), SPT_LA(45),
+    SPT_LA(46), SPT_LA(47), SPT_LA(48), SPT_LA(49), SPT_LA(50), SPT_LA(51), SPT_LA(52), SPT_LA(53), SPT_LA(54),
+    SPT_LA(55), SPT_LA(56), SPT_LA(57), SPT_LA(58), SPT_LA(59), SPT_LA(60), SPT_LA(61), SPT_LA(62), SPT_LA(63)};
+#undef SPT_LA
+static __device__ __constant__ double kLegB[64] = {
+#define SPT_LB(n) (n) / ((n) + 1.0)
+    SPT_LB(0), SPT_LB(1), SPT_LB(2), SPT_LB(3), SPT_LB(4), SPT_LB(5), SPT_LB(6), SPT_LB(7), SPT_LB(8), SPT_LB(9),
+    SPT_LB(10), SPT_LB(11), SPT_LB(12), SPT_LB(13), SPT_LB(14), SPT_LB(15), SPT_LB(16), SPT_LB(17), SPT_LB(18),
+    SPT_LB(19), SPT_LB(20), SPT_LB(21), SPT_LB(22), SPT_LB(23), SPT_LB(24), SPT_LB(25), SPT_LB(26), SPT_LB(27),
+    SPT_LB(28), SPT_LB(29), SPT_LB(30), SPT_LB(31), SPT_LB(32), SPT_LB(33), SPT_LB(34), SPT_LB(35), SPT_LB(36),
+    SPT_LB(37), SPT_LB(38), SPT_LB(39), SPT_LB(40), SPT_LB(41), SPT_LB(42), SPT_LB(43), SPT_LB(44), SPT_LB(45),
+    SPT_LB(46), SPT_LB(47), SPT_LB(48), SPT_LB(49), SPT_LB(50), SPT_LB(51), SPT_LB(52), SPT_LB(53), SPT_LB(54),
+    SPT_LB(55), SPT_LB(56), SPT_LB(57), SPT_LB(58), SPT_LB(59), SPT_LB(60), SPT_LB(61), SPT_LB(62), SPT_LB(63)};
+#undef SPT_LB
+
+// Field (E_rho, E_z) at (rho, z) of a cluster from its record (z_c, r_max,
+// M_0 .. M_(nt-1)): with r, u = cos(theta), s = sin(theta) about (0, z_c) and
+// x = r_max / r, the potential (1/4 pi) sum_n M_n x^n P_n(u) / r gives
+// E_r = (1/4 pi r^2) sum (n+1) M_n x^n P_n(u), E_theta = (s/4 pi r^2) sum
+// M_n x^n P_n'(u), turned into (rho, z) components.  P_n' by
+// P'_(n+1) = P'_(n-1) + (2n+1) P_n.
+__device__ __forceinline__ void cluster_field(const double* rec, int nt, double rho, double z, double& er,
+                                              double& ez) {
+    const double dz = z - __ldg(rec);
+    const double r2 = rho * rho + dz * dz;
+    const double ir = rsqrt(r2);
+    const double u = dz * ir, s = rho * ir, x = __ldg(rec + 1) * ir;
+    double p0 = 1.0, p1 = u, d0 = 0.0, d1 = 1.0;
+    double A = __ldg(rec + 2), B = 0.0;
+    double xn = x;
+    for (int n = 1; n < nt; ++n) {
+        const double m = __ldg(rec + 2 + n) * xn;
+        A = fma((double)(n + 1) * m, p1, A);
+        B = fma(m, d1, B);
+        const double p2 = fma(kLegA[n] * u, p1, -kLegB[n] * p0);
+        const double d2 = fma((double)(2 * n + 1), p1, d0);
+        p0 = p1;
+        p1 = p2;
+        d0 = d1;
+        d1 = d2;
+        xn *= x;
+    }
+    const double sc = ir * ir * 0.07957747154594767;  // 1 / (4 pi r^2)
+    const double e_r = A * sc, e_t = s * B * sc;
+    er = e_r * s + e_t * u;
+    ez = e_r * u - e_t * s;
+}
+
 constexpr int kWarpRuns = kWarpChunk / SPT_BLOCK_SEGS;
 static_assert(kWarpRuns <= 32, "one lane classifies each run of a chunk");
 
 template <int NP, int NQ, bool MIX>
-__device__ bool far_adaptive_warp(Ctx& c, int r0, int np_, unsigned long long& far_evals) {
+__device__ bool far_adaptive_warp(Ctx& c, int r0, int np_, unsigned long long& far_evals,
+                                  unsigned long long& cl_evals) {
     const SptBem& b = c.bem;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nseg = b.n_seg, nps = b.nodes_per_seg;
@@ -596,6 +653,7 @@ __device__ bool far_adaptive_warp(Ctx& c, int r0, int np_, unsigned long long& f
     int* R3 = R2 + kWarpRuns;
     int* M = R3 + kWarpRuns;
     int* Mcls = M + kWarpRuns;
+    unsigned* covered = reinterpret_cast<unsigned*>(Mcls + kWarpRuns);  // runs summed by cluster expansions
     double pr[NP], pinv[NP], pz[NP], ar[NP], az[NP];
     float fr[NP], fz[NP], kr[NP], kz[NP], prf[NP], pinvf[NP];
     float sa[NP];
@@ -617,12 +675,47 @@ __device__ bool far_adaptive_warp(Ctx& c, int r0, int np_, unsigned long long& f
     const double* cw = b.coarse + 2 * b.coarse_stride;
     const bool run_rule = b.blk && b.run_nodes && b.ratio_run > 0.0;
     const unsigned lt = (1u << lane) - 1u;
+    // Cluster expansions (one point per task): lane = run; the run is covered
+    // by its highest ancestor cluster that is at least kappa radii away, and
+    // the lane of the cluster's first run adds that cluster's expansion.
+    const int n_run = (nseg + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS;
+    const bool use_cl = NP == 1 && b.blk && b.clusters && b.cluster_kappa > 0.0 && n_run <= SPT_MAX_CLUSTER_RUNS;
+    if (use_cl) {
+        const int nt = b.cluster_terms, rec_len = nt + 2;
+        for (int qb = 0; qb < n_run; qb += 32) {
+            const int q = qb + lane;
+            int lv = -1, idx = 0;
+            if (q < n_run) {
+                int off = 0;
+                for (int l = 0; l < b.cluster_levels; ++l) {
+                    const int i = off + (q >> l);
+                    const double* rec = b.clusters + (size_t)i * rec_len;
+                    const double dz = pz[0] - __ldg(rec);
+                    if (pr[0] * pr[0] + dz * dz >= b.cluster_kappa * b.cluster_kappa * __ldg(rec + 1) * __ldg(rec + 1)) {
+                        lv = l;
+                        idx = i;
+                    }
+                    off += (n_run + (1 << l) - 1) >> l;
+                }
+            }
+            const unsigned cov = __ballot_sync(0xffffffffu, lv >= 0);
+            if (lane == 0) covered[qb >> 5] = cov;
+            if (lv >= 0 && (q & ((1 << lv) - 1)) == 0) {
+                double er, ez;
+                cluster_field(b.clusters + (size_t)idx * rec_len, nt, pr[0], pz[0], er, ez);
+                ar[0] += er;
+                az[0] += ez;
+                ++cl_evals;
+            }
+        }
+        __syncwarp();
+    }
     for (int c0 = 0; c0 < nseg; c0 += kWarpChunk) {
         const int q0 = c0 / SPT_BLOCK_SEGS;
         const int nr = min(kWarpRuns, (nseg - c0 + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS);
         const int q = q0 + lane;
         int cls = -1;  // 3 run rule, 2 Gauss-2 on every segment, 1 no near segment, 0 full test
-        if (lane < nr) {
+        if (lane < nr && !(use_cl && ((covered[q >> 5] >> (q & 31)) & 1u))) {
             cls = 0;
             if (b.blk) {
                 double lb = INFINITY;
@@ -942,15 +1035,15 @@ __device__ __forceinline__ void near_point(Ctx& c, int k, unsigned long long& n_
 // form, float64 again when its sum is ill-conditioned.  The float64 tile is
 // the float64 form's, so with every sum redone the mixed form reproduces it.
 template <int FORM>
-__device__ __forceinline__ void far_point(Ctx& c, int k, unsigned long long& fe) {
+__device__ __forceinline__ void far_point(Ctx& c, int k, unsigned long long& fe, unsigned long long& ce) {
     if constexpr (FORM == SPT_FORM_FP64) {
-        far_adaptive_warp<1, 8, false>(c, k, 1, fe);
+        far_adaptive_warp<1, 8, false>(c, k, 1, fe, ce);
     } else {
         // float32 tiles keep 4 ring evaluations in flight per lane (8 spill at
         // 128 registers; more resident warps supply the parallelism instead)
-        if (far_adaptive_warp<1, 4, true>(c, k, 1, fe)) {
+        if (far_adaptive_warp<1, 4, true>(c, k, 1, fe, ce)) {
             if ((threadIdx.x & 31) == 0) atomicAdd(c.cnt + SPT_CNT_FP64_ROUNDS, 1ull);
-            far_adaptive_warp<1, 8, false>(c, k, 1, fe);
+            far_adaptive_warp<1, 8, false>(c, k, 1, fe, ce);
         }
     }
 }
@@ -994,7 +1087,9 @@ __device__ __forceinline__ void bem_sums(Ctx& c, int n, int* status_flag) {
         __shared__ int s_far_task;
         if (tid == 0) s_far_task = c.nw;
         __syncthreads();
-        for (int k = warp; k < n; k = next_task(&s_far_task)) far_point<FORM>(c, k, far_evals);
+        unsigned long long cl_evals = 0;
+        for (int k = warp; k < n; k = next_task(&s_far_task)) far_point<FORM>(c, k, far_evals, cl_evals);
+        count_add(c, SPT_CNT_CLUSTER_EVALS, cl_evals);
         __syncthreads();
     } else {
         const int tile_cap = c.L.tile_cap;
@@ -1301,13 +1396,13 @@ __device__ void bem_points_fused(Ctx& c, int n) {
     __shared__ int s_task;
     if (threadIdx.x == 0) s_task = c.nw;
     __syncthreads();
-    unsigned long long n_near = 0, n_ring_near = 0, far_evals = 0;
+    unsigned long long n_near = 0, n_ring_near = 0, far_evals = 0, cl_evals = 0;
     for (int k = threadIdx.x >> 5; k < n; k = next_task(&s_task)) {
         closest_point(c, k, false);
         __syncwarp();
         near_point(c, k, n_near, n_ring_near);
         __syncwarp();
-        far_point<FORM>(c, k, far_evals);
+        far_point<FORM>(c, k, far_evals, cl_evals);
         if (lane == 0) {
             const double x = P[8 * k + 0], y = P[8 * k + 1];
             const double rho = hypot(x, y);
@@ -1326,6 +1421,7 @@ __device__ void bem_points_fused(Ctx& c, int n) {
     count_add(c, SPT_CNT_NEAR_PAIRS, n_near);
     count_add(c, SPT_CNT_RING_NEAR, n_ring_near);
     count_add(c, SPT_CNT_RING_FAR, far_evals);
+    count_add(c, SPT_CNT_CLUSTER_EVALS, cl_evals);
     __syncthreads();
 }
 

@@ -273,6 +273,18 @@ int check_bem(const SptBem* b) {
     }
     if (b->blk && b->blk_stride < (b->n_seg + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS)
         return fail(SPT_ERR_ARG, "run bounds table too small");
+    if (b->far_rule == SPT_FAR_ADAPTIVE && b->clusters && b->cluster_kappa > 0.0) {
+        const int n_run = (b->n_seg + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS;
+        int levels = 1;
+        for (int size = 1; (n_run + size - 1) / size > 1; size *= 2) ++levels;
+        if (!b->blk) return fail(SPT_ERR_ARG, "cluster expansions need the run bounds table");
+        if (n_run > SPT_MAX_CLUSTER_RUNS)
+            return fail(SPT_ERR_CAPACITY, "cluster expansions: %d runs exceed %d", n_run, SPT_MAX_CLUSTER_RUNS);
+        if (b->cluster_levels != levels)
+            return fail(SPT_ERR_ARG, "cluster table has %d levels, %d runs need %d", b->cluster_levels, n_run, levels);
+        if (b->cluster_terms < 1 || b->cluster_terms > 64) return fail(SPT_ERR_ARG, "cluster_terms must be in [1, 64]");
+        if (!(b->cluster_kappa > 1.0)) return fail(SPT_ERR_ARG, "cluster_kappa must exceed 1 (or be <= 0: off)");
+    }
     return SPT_OK;
 }
 

@@ -21,7 +21,12 @@ Built once per geometry, like the reference's per-device field cache
 * run-node table [3, n_run * 8]: the 8-point Gauss rule over the arclength
   of each whole run.  A run is flagged for it only when it is straight and,
   at probe points RATIO_RUN arclengths away, its 8-point sum matches the
-  segment-wise Gauss-4 sum to RUN_TOL.
+  segment-wise Gauss-4 sum to RUN_TOL;
+* cluster table [n_cluster, CLUSTER_TERMS + 2]: a binary tree over the runs
+  (level l: clusters of 2^l consecutive runs) with, per cluster, its centre
+  on the axis, its radius and the axisymmetric multipole moments of its
+  far-node weights, for the adaptive rule's cluster expansions.  Not in the
+  reference.
 """
 
 import ctypes
@@ -38,6 +43,10 @@ GAUSS2_X, GAUSS2_W = np.polynomial.legendre.leggauss(2)
 RATIO4, RATIO2, RATIO_RUN = 8.0, 300.0, 4.0
 RUN_TOL = 1e-10
 GAUSS_RUN_X, GAUSS_RUN_W = np.polynomial.legendre.leggauss(_lib.RUN_NODES)
+# cluster expansions: terms kept, and separation (distance from the centre
+# over the cluster's radius) beyond which a cluster is summed by them
+CLUSTER_TERMS, CLUSTER_KAPPA = 32, 3.0
+MAX_CLUSTER_RUNS = 256
 
 
 def segment_table(profile, sigma):
@@ -185,6 +194,54 @@ def run_tables(profile, sigma, block=_lib.BLOCK_SEGS, ratio_run=RATIO_RUN, tol=R
     return out, nodes
 
 
+def cluster_tables(profile, sigma, n_subdiv, n_terms=CLUSTER_TERMS, block=_lib.BLOCK_SEGS):
+    """(table [n_cluster, n_terms + 2], n_levels).  Level l holds
+    ceil(n_run / 2^l) clusters of 2^l consecutive runs (the last one shorter),
+    levels one after another, up to the level with a single cluster.  Record:
+    centre z_c (on the axis: the middle of the cluster's z range), radius
+    r_max (largest distance from (0, z_c) to an end of its segments, which
+    bounds every ring of the cluster), moments M_n = sum_q w_q (r_q/r_max)^n
+    P_n(u_q) over its far nodes q, with r_q, u_q the distance from (0, z_c) and
+    the cosine of the polar angle (the potential of a ring about a centre on
+    the axis is sum_n r'^n / r^(n+1) P_n(u') P_n(u), the addition theorem's
+    axisymmetric term)."""
+    prof = np.asarray(profile, dtype=np.float64)
+    rq, zq, aq, sq = far_nodes(prof, sigma, n_subdiv)
+    wq = aq * sq
+    n_seg = len(prof) - 1
+    per = 4 * n_subdiv
+    n_run = (n_seg + block - 1) // block
+    rows = []
+    levels = 0
+    size = 1
+    while True:
+        n_cl = (n_run + size - 1) // size
+        for k in range(n_cl):
+            s0, s1 = k * size * block, min((k + 1) * size * block, n_seg)
+            ends = prof[s0:s1 + 1]
+            zc = 0.5 * (ends[:, 1].min() + ends[:, 1].max())
+            rmax = np.sqrt(ends[:, 0] ** 2 + (ends[:, 1] - zc) ** 2).max()
+            r, z, w = rq[s0 * per:s1 * per], zq[s0 * per:s1 * per], wq[s0 * per:s1 * per]
+            rr = np.sqrt(r * r + (z - zc) ** 2)
+            u = np.where(rr > 0.0, (z - zc) / np.where(rr > 0.0, rr, 1.0), 1.0)
+            x = rr / rmax
+            M = np.zeros(n_terms)
+            p_prev, p = np.ones_like(u), u
+            xn = np.ones_like(u)
+            for n in range(n_terms):
+                pn = p_prev if n == 0 else p
+                M[n] = np.sum(w * xn * pn)
+                if n >= 1:
+                    p_prev, p = p, ((2 * n + 1) * u * p - n * p_prev) / (n + 1)
+                xn = xn * x
+            rows.append(np.concatenate([[zc, rmax], M]))
+        levels += 1
+        if n_cl == 1:
+            break
+        size *= 2
+    return np.array(rows), levels
+
+
 class BemTables:
     """Segment and far-node tables on a CUDA device, plus the SptBem view."""
 
@@ -218,6 +275,12 @@ class BemTables:
         self.blk = torch.as_tensor(blk, device=device)
         self.run_nodes = torch.as_tensor(rn, device=device)
         self.n_run_rule = int(blk[5].sum())
+        n_run = blk.shape[1]
+        self.clusters = None
+        if n_run <= MAX_CLUSTER_RUNS:
+            ct, levels = cluster_tables(self.profile, self.sigma, self.n_subdiv)
+            self.clusters = torch.as_tensor(np.ascontiguousarray(ct), device=device)
+            self.cluster_levels = levels
         self.struct = _lib.SptBem()
         s = self.struct
         s.n_seg = n_seg
@@ -238,18 +301,28 @@ class BemTables:
         s.ratio_run = RATIO_RUN
         s.run_nodes = self.run_nodes.data_ptr()
         s.run_stride = self.run_nodes.shape[1]
+        if self.clusters is not None:
+            s.clusters = self.clusters.data_ptr()
+            s.cluster_levels = self.cluster_levels
+            s.cluster_terms = CLUSTER_TERMS
+            s.cluster_kappa = CLUSTER_KAPPA
 
-    def view(self, far_rule="reference", ratio4=RATIO4, ratio2=RATIO2, ratio_run=RATIO_RUN, bounds=True):
+    def view(self, far_rule="reference", ratio4=RATIO4, ratio2=RATIO2, ratio_run=RATIO_RUN, bounds=True,
+             cluster_kappa=None):
         """An SptBem over these tables with the given far rule (the tables
         must outlive it); ratio_run <= 0 turns the run rule off; bounds=False
         leaves out the run bounds, so every per-point scan visits every
-        segment (and the run rule is off)."""
+        segment (and the run rule and the clusters are off);
+        cluster_kappa <= 0 turns the cluster expansions off."""
         v = _lib.SptBem()
         ctypes.pointer(v)[0] = self.struct
         v.far_rule = _lib.FAR_RULES[far_rule] if isinstance(far_rule, str) else int(far_rule)
         v.ratio4, v.ratio2, v.ratio_run = float(ratio4), float(ratio2), float(ratio_run)
+        if cluster_kappa is not None:
+            v.cluster_kappa = float(cluster_kappa)
         if not bounds:
             v.blk, v.blk_stride = None, 0
+            v.clusters, v.cluster_kappa = None, 0.0
         return v
 
     @property

@@ -67,6 +67,7 @@ METRIC = "accepted RK45 particle-steps/s at ≤1e-6 rel endpoint err: chosen for
 UNIT = "particle-steps/s"
 FLOP_PER_RING = 64.0   # nominal FLOPs of one ring-kernel evaluation (26 algebra + 38 for K, E)
 FLOP_PER_PAIR = 20.0   # nominal FLOPs of one softened pair interaction
+FLOP_PER_CLUSTER = 12.0 * 32  # nominal FLOPs of one 32-term cluster expansion (12 per term)
 WHOLE_TRACE = 1_000_000  # attempt budget of a whole-trace launch (every group reaches t_end far sooner)
 T_END = dict(c0=None, c1=20e-12, c2=20e-12, c3=30e-12, c4=20e-12)
 
@@ -475,7 +476,8 @@ def run_gpu(args, rank, world):
     if rank == 0 and not args.no_plain and (args.form, args.far_rule) != ("fp64", "reference"):
         plain, acc = plain_and_accuracy(args, wl, pos, vel, tb, q, m, sizes, dev, t_max, budget)
     peak = (fp64_peak_tflops if args.form == "fp64" else fp32_peak_tflops)(torch, dev) if rank == 0 else None
-    flops = dc["ring_far"] * FLOP_PER_RING + dc["ring_near"] * FLOP_PER_RING + dc["pair_evals"] * FLOP_PER_PAIR
+    flops = (dc["ring_far"] * FLOP_PER_RING + dc["ring_near"] * FLOP_PER_RING + dc["pair_evals"] * FLOP_PER_PAIR
+             + dc["cluster_evals"] * FLOP_PER_CLUSTER)
     achieved = flops / t_total / 1e12
     return dict(value=steps_all / t_max_ranks, live=live_all / t_max_ranks, t_total=t_max_ranks, times=times,
                 counters=dc, clocks=clk.summary(), e2e=e2e, peak=peak, achieved=achieved, config=wl["config"],
@@ -669,7 +671,8 @@ def main():
                       peak_source=("measured in-run: cuBLAS DGEMM 4096^3" if fp64 else
                                    "measured in-run: cuBLAS SGEMM 8192^3, TF32 off")
                       + " (no FP32/FP64 figure in the measured-peaks file)",
-                      flop_model=f"{FLOP_PER_RING:g} FLOP/ring eval, {FLOP_PER_PAIR:g} FLOP/pair (nominal)"),
+                      flop_model=f"{FLOP_PER_RING:g} FLOP/ring eval, {FLOP_PER_PAIR:g} FLOP/pair, "
+                                 f"{FLOP_PER_CLUSTER:g} FLOP/cluster expansion (nominal)"),
         plain_fp64=r["plain"],
         accuracy=r["accuracy"],
         counters=r["counters"],

@@ -77,7 +77,8 @@ extern "C" {
 #define SPT_CNT_FP64_TARGETS 9       /* mixed form: pair-sum targets recomputed in float64 */
 #define SPT_CNT_LIVE_STEPS 10        /* sum over accepted group-steps of the particles alive (born, not
                                         killed) at the step start */
-#define SPT_N_COUNTERS 11
+#define SPT_CNT_CLUSTER_EVALS 11     /* cluster-expansion evaluations of the adaptive far rule */
+#define SPT_N_COUNTERS 12
 
 /* Geometry parameters.  Fields a kind does not use are ignored. */
 typedef struct {
@@ -150,7 +151,27 @@ typedef struct {
     double ratio_run;
     const double* run_nodes;
     int64_t run_stride;
+    /* Cluster expansions (adaptive far rule with blk only; no counterpart in
+     * the reference): a binary tree over the runs -- level 0 the runs, level
+     * l the clusters of 2^l consecutive runs, ceil(n_run / 2^l) of them,
+     * levels stored one after another -- with, per cluster, a record of
+     * cluster_terms + 2 doubles: the centre z_c on the axis, the radius
+     * r_max of the sphere about (0, z_c) that holds all its rings, and the
+     * axisymmetric multipole moments M_n = sum_q w_q (r_q / r_max)^n
+     * P_n(cos theta_q) of its reference nodes (n < cluster_terms).  A run
+     * whose cluster at some level is at least cluster_kappa * r_max from the
+     * point is summed by the highest such cluster's expansion
+     * E = -grad (1/4 pi) sum_n M_n r_max^n P_n(cos theta) / r^(n+1), which
+     * matches the reference nodes' sum to ~1e-15 of the cluster's field at
+     * kappa 3, 32 terms.  cluster_kappa <= 0 or clusters NULL: off.
+     * At most SPT_MAX_CLUSTER_RUNS runs, 64 terms. */
+    const double* clusters;
+    int32_t cluster_levels;
+    int32_t cluster_terms;
+    double cluster_kappa;
 } SptBem;
+
+#define SPT_MAX_CLUSTER_RUNS 256
 
 #define SPT_RUN_NODES 8
 

@@ -202,15 +202,95 @@ def _adaptive_override(er_s, ez_s, rho_e, z_e, dist, seg, coarse, ratio4, ratio2
                 ez_s[p, js] = np.sum(wq[js] * ez, axis=-1)
 
 
+def cluster_table(profile, sigma, n_subdiv=8, n_terms=32, block=32):
+    """Cluster expansions of the adaptive rule (not in the reference; the
+    product's tables restate this): a binary tree over the runs of `block`
+    segments, level l the clusters of 2^l consecutive runs, each with its
+    centre (0, z_c) (the middle of its z range), the radius r_max of the
+    sphere about it through its farthest segment end, and the moments
+    M_n = sum_q w_q (r_q / r_max)^n P_n(cos theta_q) of its far nodes (the
+    axisymmetric term of the addition theorem: a ring's potential about a
+    centre on the axis is sum_n r'^n / r^(n+1) P_n(u') P_n(u)).  Returns a
+    list of levels, each a list of (z_c, r_max, M, s0, s1)."""
+    from scipy.special import eval_legendre
+    profile = np.asarray(profile, dtype=float)
+    rq, zq, aq, sq = far_nodes(profile, sigma, n_subdiv)
+    wq = aq * sq
+    n_seg = len(profile) - 1
+    per = 4 * n_subdiv
+    n_run = (n_seg + block - 1) // block
+    levels, size = [], 1
+    while True:
+        n_cl = (n_run + size - 1) // size
+        lev = []
+        for k in range(n_cl):
+            s0, s1 = k * size * block, min((k + 1) * size * block, n_seg)
+            ends = profile[s0:s1 + 1]
+            zc = 0.5 * (ends[:, 1].min() + ends[:, 1].max())
+            rmax = np.sqrt(ends[:, 0] ** 2 + (ends[:, 1] - zc) ** 2).max()
+            r, z, w = rq[s0 * per:s1 * per], zq[s0 * per:s1 * per], wq[s0 * per:s1 * per]
+            rr = np.hypot(r, z - zc)
+            u = (z - zc) / rr
+            M = np.array([np.sum(w * (rr / rmax) ** n * eval_legendre(n, u)) for n in range(n_terms)])
+            lev.append((zc, rmax, M, s0, s1))
+        levels.append(lev)
+        if n_cl == 1:
+            return levels
+        size *= 2
+
+
+def cluster_field(zc, rmax, M, rho, z):
+    """(E_rho, E_z) of a cluster's expansion at (rho, z):
+    E = -grad (1/4 pi) sum_n M_n rmax^n P_n(u) / r^(n+1)."""
+    from scipy.special import eval_legendre
+    dz = z - zc
+    r = np.hypot(rho, dz)
+    u, s = dz / r, rho / r
+    n = np.arange(len(M))
+    x = (rmax / r) ** n
+    P = eval_legendre(n, u)
+    # P_n'(u) by P'_(n+1) = P'_(n-1) + (2n+1) P_n
+    D = np.zeros(len(M))
+    for k in range(1, len(M)):
+        D[k] = (D[k - 2] if k >= 2 else 0.0) + (2 * k - 1) * P[k - 1]
+    e_r = np.sum((n + 1) * M * x * P) / (4 * np.pi * r * r)
+    e_t = s * np.sum(M * x * D) / (4 * np.pi * r * r)
+    return e_r * s + e_t * u, e_r * u - e_t * s
+
+
+def _cluster_override(er_s, ez_s, rho_e, z_e, levels, kappa, block=32):
+    """Cluster rule: for each point, every run takes its highest ancestor
+    cluster at least kappa r_max from the point; the segments of a covered
+    cluster give way to its expansion (kept in its first segment's slot)."""
+    n_seg = er_s.shape[1]
+    n_run = (n_seg + block - 1) // block
+    for p in range(len(rho_e)):
+        cover = {}
+        for q in range(n_run):
+            best = None
+            for l, lev in enumerate(levels):
+                zc, rmax, M, s0, s1 = lev[q >> l]
+                if np.hypot(rho_e[p], z_e[p] - zc) >= kappa * rmax:
+                    best = (l, q >> l)
+            if best is not None:
+                cover[best] = levels[best[0]][best[1]]
+        for (l, k), (zc, rmax, M, s0, s1) in cover.items():
+            er_s[p, s0:s1] = 0.0
+            ez_s[p, s0:s1] = 0.0
+            er_s[p, s0], ez_s[p, s0] = cluster_field(zc, rmax, M, rho_e[p], z_e[p])
+
+
 def field(points, profile, sigma, n_subdiv=8, chunk=256, far_rule="reference", ratio4=8.0, ratio2=300.0,
-          round_size=1, run_flags=None, ratio_run=4.0):
+          round_size=1, run_flags=None, ratio_run=4.0, clusters=None, cluster_kappa=3.0):
     """bem/axisymmetric.py:501-605 -- E = -grad S[sigma] at points (..., 3).
 
     far_rule="adaptive" swaps the sub-panel sums of distant segments for the
     whole-segment rules of ``_adaptive_override`` (chunk must be a multiple
     of round_size so rounds are consecutive points of the input), and, with
     ``run_flags`` (which runs of 32 segments may take it), distant flagged
-    runs for the run rule of ``_run_override``."""
+    runs for the run rule of ``_run_override``, and, with ``clusters`` (a
+    ``cluster_table``), runs covered by a distant cluster for its expansion
+    (``_cluster_override``)."""
     points = np.asarray(points, dtype=float)
     shape = points.shape
     flat = points.reshape(-1, 3)
@@ -250,6 +330,8 @@ def field(points, profile, sigma, n_subdiv=8, chunk=256, far_rule="reference", r
             _adaptive_override(er_s, ez_s, rho_e, z, dist, seg, coarse, ratio4, ratio2, round_size)
             if runs is not None:
                 _run_override(er_s, ez_s, rho_e, z, runs, run_flags, ratio_run, round_size)
+            if clusters is not None:
+                _cluster_override(er_s, ez_s, rho_e, z, clusters, cluster_kappa)
         pi, si = np.nonzero(dist < seg["length"][None, :])
         for p, s in zip(pi, si):
             d = max(dist[p, s], 1e-15 * seg["length"][s])

@@ -30,7 +30,8 @@ def test_bem_field_adaptive_fp64(fixture):
     tab = BemTables(g["profile"], g["sigma"], int(g["n_subdiv"]))
     e = engine.bem_field(tab, g["points"], far_rule="adaptive").cpu().numpy()
     ora = ob.field(g["points"], g["profile"], g["sigma"], int(g["n_subdiv"]), far_rule="adaptive",
-                   run_flags=tab.blk[5].cpu().numpy() > 0)
+                   run_flags=tab.blk[5].cpu().numpy() > 0,
+                   clusters=ob.cluster_table(g["profile"], g["sigma"], int(g["n_subdiv"])))
     # near-surface fixture points lose digits to cancellation (the reference
     # rule's parity test allows 1e-10 for the same reason)
     assert _rel_rows(e, ora).max() < 1e-11
@@ -47,7 +48,9 @@ def test_bem_field_adaptive_mixed(fixture):
 
 def test_bem_field_adaptive_benchmark_tip():
     """2000-segment tip: kernel (both rules) against the oracle's adaptive
-    rule at points 2 nm .. 10 um from the apex, rounds of mixed distances."""
+    rule (run rule and cluster expansions included) at points 2 nm .. 10 um
+    from the apex; the rule without the run rule, and without the cluster
+    expansions, against the reference rule."""
     g = load_golden("sigma_c1")
     prof, sig = g["profile"], g["sigma"]
     apex = prof[:, 1].max()
@@ -61,12 +64,16 @@ def test_bem_field_adaptive_benchmark_tip():
     assert tab.n_run_rule > 40  # the straight wall runs
     ada = engine.bem_field(tab, pts, far_rule="adaptive").cpu().numpy()
     seg_only = engine.bem_field(tab, pts, far_rule="adaptive", ratio_run=0.0).cpu().numpy()
+    no_cl = engine.bem_field(tab, pts, far_rule="adaptive", cluster_kappa=0.0).cpu().numpy()
     ref = engine.bem_field(tab, pts).cpu().numpy()
-    ora = ob.field(pts, prof, sig, 8, far_rule="adaptive", run_flags=tab.blk[5].cpu().numpy() > 0)
+    ora = ob.field(pts, prof, sig, 8, far_rule="adaptive", run_flags=tab.blk[5].cpu().numpy() > 0,
+                   clusters=ob.cluster_table(prof, sig))
     norm = np.linalg.norm(ora, axis=-1)
     assert (np.abs(ada - ora).max(axis=-1) / norm).max() < 1e-12
     assert (np.abs(ada - ref).max(axis=-1) / norm).max() < 1e-12
     assert (np.abs(seg_only - ref).max(axis=-1) / norm).max() < 1e-12
+    assert (np.abs(no_cl - ref).max(axis=-1) / norm).max() < 1e-12
+    assert not np.array_equal(no_cl, ada)  # the expansions did take part
 
 
 def _tip_points(n, seed):
