@@ -34,7 +34,7 @@ torch = pytest.importorskip("torch")
 if not torch.cuda.is_available():
     pytest.skip("needs a CUDA device", allow_module_level=True)
 
-from bem_b200 import engine  # noqa: E402
+from bem_b200 import _lib, engine  # noqa: E402
 
 import gpu_util as gu  # noqa: E402
 
@@ -84,6 +84,13 @@ def _run(spec, fixtures, form, budget_first=None, binned=False):
         else:
             tr.launch(batch, prm)
         snaps["budget"] = snap()
+        # the budget-cut groups stop here; only the others go on to t_max
+        g0 = 0
+        for f in fixtures:
+            G = f["pos0"].shape[0]
+            if int(f["max_attempts"]) > 0:
+                batch.status[g0:g0 + G] = _lib.GROUP_DONE
+            g0 += G
     if any(int(f["max_attempts"]) <= 0 for f in fixtures):
         tr.run(batch, t_max, rtol, atol, 1e-12, gu.CM, bins=plan)
         snaps["done"] = snap()
