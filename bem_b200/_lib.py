@@ -36,13 +36,19 @@ class SptGeometry(ctypes.Structure):
                 ("z_max", _d), ("z_handoff", _d), ("bottom_fillet", _d), ("rim_fillet", _d)]
 
 
+class SptImage(ctypes.Structure):
+    _fields_ = [("n_nodes", _i32), ("n_max", _i32), ("n_quad", _i32), ("mirror_symmetric", _i32),
+                ("node", _p), ("seg", _p), ("quad", _p), ("a_inv", _p), ("rho_floor", _d), ("d_lo", _d),
+                ("d_hi", _d)]
+
+
 class SptBem(ctypes.Structure):
     _fields_ = [("n_seg", _i32), ("nodes_per_seg", _i32), ("seg_stride", _i64), ("node_stride", _i64),
                 ("seg", _p), ("node", _p), ("gauss8_x", _d * 8), ("gauss8_w", _d * 8),
                 ("far_rule", _i32), ("reserved", _i32), ("ratio4", _d), ("ratio2", _d), ("coarse", _p),
                 ("coarse_stride", _i64), ("blk", _p), ("blk_stride", _i64), ("ratio_run", _d), ("run_nodes", _p),
                 ("run_stride", _i64), ("clusters", _p), ("cluster_levels", _i32), ("cluster_terms", _i32),
-                ("cluster_kappa", _d)]
+                ("cluster_kappa", _d), ("image", SptImage)]
 
 
 class SptState(ctypes.Structure):
@@ -80,6 +86,9 @@ class SptGemmArgs(ctypes.Structure):
                 ("status", _p)]
 
 
+IMAGE_MAX_MODES = 64
+TRACE_IMAGE_MODES = 16
+ABI_VERSION = 3
 EPI_STORE, EPI_BIAS_SILU, EPI_DSILU = 0, 1, 2
 _f = ctypes.c_float
 
@@ -107,6 +116,10 @@ SIGNATURES = {
     "spt_mlp_colsum": (ctypes.c_int, [_p, _i64, _p, _p, _p, _p]),
     "spt_mlp_reduce_splits": (ctypes.c_int, [_p, _i32, _i64, _p, _p]),
     "spt_mlp_adam": (ctypes.c_int, [_p, _p, _p, _p, _i64, _f, _f, _f, _f, _i32, _p, _p, _p]),
+    "spt_toroidal_q": (ctypes.c_int, [_p, _i64, _i32, _p, _p, _p]),
+    "spt_image_assemble": (ctypes.c_int, [_p, _p, _i32, _i32, _d, _d, _i32, _p, _p, _p, _p]),
+    "spt_image_force": (ctypes.c_int, [_p, _p, _p, _p, _p, _p, _i32, _i32, ctypes.POINTER(SptImage),
+                                       ctypes.POINTER(SptGeometry), _d, _d, _p, _p, _p, _p]),
     "spt_trace_noalloc": (ctypes.c_int, [ctypes.POINTER(SptState), ctypes.POINTER(SptTraceParams),
                                          ctypes.POINTER(SptGeometry), ctypes.POINTER(SptBem), _p]),
 }

@@ -14,9 +14,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libspt_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in (
-    "spt_kernels.cu", "spt_mlp.cu", "spt_trace_flat.cu", "spt_trace_tip.cu", "spt_trace_tipbem.cu",
+    "spt_kernels.cu", "spt_mlp.cu", "spt_image.cu", "spt_trace_flat.cu", "spt_trace_tip.cu", "spt_trace_tipbem.cu",
     "spt_trace_well.cu", "spt_trace_post.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", h) for h in ("spt_device.cuh", "spt_math.cuh", "spt_umma.cuh")] + [
+DEPS = SOURCES + [os.path.join(HERE, "csrc", h) for h in ("spt_device.cuh", "spt_math.cuh", "spt_umma.cuh", "spt_abi.hpp")] + [
     os.path.join(REPO, "include", "spt_b200.h")]
 OBJ_DIR = os.path.join(HERE, "_build")
 

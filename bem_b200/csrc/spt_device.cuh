@@ -11,6 +11,7 @@
 #include <type_traits>
 
 #include "../../include/spt_b200.h"
+#include "spt_image.cuh"
 #include "spt_math.cuh"
 #include "spt_umma.cuh"
 
@@ -172,6 +173,7 @@ struct Layout {
     int fld;                  // 3E field
     int img;                  // 4E sphere images
     int bpt;                  // 8E per BEM list entry: x y z rho_e z_e near_r near_z (+1 pad)
+    int imgs;                 // scratch of the BEM image-charge force (geometries with z0), or 0 doubles
     int sur;                  // surrogate region: act (4096), wt (4096), sout 2E, sseg E, st E, sd E, feat 128; -1 if none
     int tiles;                // reference far rule: 2 * 3 * tile_cap node tiles; adaptive: per-warp scratch
     int tile_cap;             // nodes per TMA tile row (reference far rule)
@@ -199,7 +201,7 @@ static_assert(kWarpScratchInts % 2 == 0, "per-warp scratch keeps 8-byte alignmen
 // warp of a CTA of `warps` warps.  want_tiles false: neither (paths that
 // evaluate no far sum).
 __host__ __device__ inline Layout make_layout(int E, int far_rule, bool want_sur = false, bool want_tiles = true,
-                                              int warps = kMaxWarps) {
+                                              int warps = kMaxWarps, int img_doubles = 0) {
     Layout L;
     const bool big = E > kSmallGroup;
     int o = 0;
@@ -221,6 +223,7 @@ __host__ __device__ inline Layout make_layout(int E, int far_rule, bool want_sur
     L.fld = o; o += 3 * E;
     L.img = o; o += 4 * E;
     L.bpt = o; o += 8 * E;
+    L.imgs = o; o += img_doubles;
     if (want_sur) {
         o = (o + 127) & ~127;  // 1 KiB alignment for the tensor-core operand tiles
         L.sur = o; o += 8192 + 5 * E + 128;
@@ -248,6 +251,22 @@ __host__ __device__ inline Layout make_layout(int E, int far_rule, bool want_sur
     return L;
 }
 
+// Partial right-hand sides of the image-charge solve per profile node: as
+// many source subsets as the CTA has threads per node, 1 to 4.
+__host__ __device__ inline int image_chunks(int P, int threads) {
+    const int c = threads / (P > 0 ? P : 1);
+    return c < 1 ? 1 : (c > 4 ? 4 : c);
+}
+
+// Shared doubles the BEM image-charge force needs for groups of up to E
+// particles on a CTA of `threads` threads: 0 unless the geometry is a BEM
+// tip or well built with z0 and the image tables are given.
+__host__ __device__ inline int image_scratch(const SptGeometry& g, const SptBem& b, int E, int threads) {
+    if (!(g.kind == SPT_GEOM_TIP_BEM || g.kind == SPT_GEOM_WELL_BEM) || !g.has_image || b.image.n_nodes < 2) return 0;
+    return (int)spt_img::scratch_doubles(E, b.image.mirror_symmetric, b.image.n_nodes, b.image.n_max,
+                                         image_chunks(b.image.n_nodes, threads));
+}
+
 // global per-CTA slot for big groups: y0 6E, nw 6E, kp 21E, kv 21E
 __host__ __device__ inline size_t big_slot_doubles(int E) { return (size_t)54 * E; }
 
@@ -266,7 +285,7 @@ struct Ctx {
     int E;
     double* base;    // dynamic smem
     Layout L;
-    double *y0, *nw_, *sp, *kp, *kv, *tb, *td, *q, *m, *cps, *fld, *img, *bpt, *tiles, *red;
+    double *y0, *nw_, *sp, *kp, *kv, *tb, *td, *q, *m, *cps, *fld, *img, *bpt, *tiles, *red, *imgs;
     int* live;
     int* list;
     unsigned char* nflag;
@@ -300,7 +319,7 @@ __device__ inline void bind(Ctx& c, double* smem, int E, int far_rule, double* s
     c.E = E;
     c.nt = blockDim.x;
     c.nw = blockDim.x >> 5;
-    c.L = make_layout(E, far_rule, sur, true, blockDim.x >> 5);
+    c.L = make_layout(E, far_rule, sur, true, blockDim.x >> 5, image_scratch(c.g, c.bem, E, blockDim.x));
     c.round_pts = kRound;
     c.kappa = kKappa;
     c.cnt = s_cnt;
@@ -325,6 +344,7 @@ __device__ inline void bind(Ctx& c, double* smem, int E, int far_rule, double* s
     c.fld = smem + L.fld;
     c.img = smem + L.img;
     c.bpt = smem + L.bpt;
+    c.imgs = smem + L.imgs;
     c.tiles = smem + L.tiles;
     c.red = smem + L.red;
     int* ib = reinterpret_cast<int*>(smem + L.ints);
@@ -1498,6 +1518,26 @@ __device__ __forceinline__ double group_sum(double v, int T) {
 // live particles (geometry.py:289-299).  Positions in c.sp (3E), result in
 // out (3 arrays of stride E... stored as out[0*E+i], out[E+i], out[2E+i]).
 
+// BEM image-charge force on the stage positions c.sp of the group, into
+// c.img (fx, fy, fz: 3E), from the image tables in c.bem.image.  Out of line:
+// its per-mode register arrays stay out of the stage code's allocation.
+static __device__ __noinline__ void stage_image_force(Ctx& c) {
+    __shared__ int s_imgflag;
+    const int E = c.E;
+    const double* sx = c.sp;
+    spt_img::ImgParams ip = spt_img::image_params(c.bem.image, &c.g, c.kc, 0.0);
+    ip.soft2 = c.soft2;
+    ip.chunks = image_chunks(c.bem.image.n_nodes, c.nt);
+    auto load = [&](int i, double& x, double& y, double& z, double& q) {
+        x = sx[i];
+        y = sx[E + i];
+        z = sx[2 * E + i];
+        q = c.live[i] ? c.q[i] : 0.0;
+    };
+    spt_img::group_force<SPT_TRACE_IMAGE_MODES>(c.bem.image, ip, E, load, c.imgs, c.img, c.img + E, c.img + 2 * E,
+                                                 &s_imgflag);
+}
+
 template <int KIND, int FORM, int FAR>
 __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
     const int E = c.E, tid = threadIdx.x;
@@ -1553,6 +1593,15 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
             c.fld[3 * i + 2] = c.bpt[8 * k + 7];
         }
         __syncthreads();
+    }
+
+    // 1b. BEM image-charge force of a tip or well built with z0
+    // (bem/geometry.py:326-344, 780-797; bem/image_charge.py:816-1056):
+    // the group's joint mode solve, into c.img (fx, fy, fz: 3E)
+    bool bem_img = false;
+    if constexpr (KIND == SPT_GEOM_TIP_BEM || KIND == SPT_GEOM_WELL_BEM) {
+        bem_img = g.has_image && c.bem.image.n_nodes >= 2;
+        if (bem_img) stage_image_force(c);
     }
 
     // 2. image sources for the sphere-on-plane construction (forces.py:170-183)
@@ -1653,6 +1702,14 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
         double fcx, fcy, fcz, fix, fiy, fiz, sabs;
         pass(std::integral_constant<bool, mix>{}, act, fcx, fcy, fcz, fix, fiy, fiz, sabs);
         reduce(fcx, fcy, fcz, fix, fiy, fiz, sabs);
+        auto bem_image = [&]() {  // the BEM image force of 1b takes the place of a pair-sum image
+            if (bem_img && act && sub == 0) {
+                fix = c.img[i];
+                fiy = c.img[E + i];
+                fiz = c.img[2 * E + i];
+            }
+        };
+        bem_image();
         double ex = 0.0, ey = 0.0, ez = 0.0;
         if (act && sub == 0) {
             if (KIND == SPT_GEOM_FLAT) {
@@ -1693,6 +1750,7 @@ __device__ void stage_accel(Ctx& c, double* out, int* status_flag) {
         if (mix && __any_sync(0xffffffffu, redo)) {
             pass(std::integral_constant<bool, false>{}, act && redo, fcx, fcy, fcz, fix, fiy, fiz, sabs);
             reduce(fcx, fcy, fcz, fix, fiy, fiz, sabs);
+            bem_image();
             if (act && redo && sub == 0) {
                 accel_of(ax, ay, az);
                 ++redone;
@@ -2202,9 +2260,9 @@ struct TraceLaunch {
 
 // Shared memory and grid of a trace launch; returns 0 or a cudaError_t.
 template <int KIND, int FORM, int FAR>
-int trace_grid(int max_group_size, int threads, int n_groups, long long max_slots, size_t* smem, int* grid,
-               int* per_sm) {
-    const Layout L = make_layout(max_group_size, FAR, FORM == SPT_FORM_SURROGATE, true, threads / 32);
+int trace_grid(int max_group_size, int threads, int n_groups, long long max_slots, int img_doubles, size_t* smem,
+               int* grid, int* per_sm) {
+    const Layout L = make_layout(max_group_size, FAR, FORM == SPT_FORM_SURROGATE, true, threads / 32, img_doubles);
     auto kern = trace_kernel<KIND, FORM, FAR>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
     if (e != cudaSuccess) return (int)e;
@@ -2228,7 +2286,8 @@ int trace_launch(const TraceLaunch& t, int grid, size_t smem) {
 
 template <int KIND, int FORM, int FAR>
 int accel_launch(const SptAccelArgs* a, const SptGeometry* g, const SptBem& bem, cudaStream_t stream) {
-    const Layout L = make_layout(a->max_group_size, FAR, false);
+    const Layout L = make_layout(a->max_group_size, FAR, false, true, kMaxWarps,
+                                 image_scratch(*g, bem, a->max_group_size, kMaxThreads));
     auto kern = accel_kernel<KIND, FORM, FAR>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
     if (e != cudaSuccess) return (int)e;
@@ -2245,9 +2304,10 @@ template <int KIND>
 int trace_dispatch(const TraceLaunch& t, int form, int far, bool launch, int* grid, size_t* smem, int* per_sm) {
     constexpr bool kBem = KIND == SPT_GEOM_TIP_BEM || KIND == SPT_GEOM_WELL_BEM || KIND == SPT_GEOM_POST_BEM;
     const int n = t.s->n_groups, E = t.s->max_group_size;
+    const int img = image_scratch(*t.g, t.bem, E, t.threads);
 #define SPT_TRACE_CASE(F, R)                                                                            \
     {                                                                                                   \
-        int rc = trace_grid<KIND, F, R>(E, t.threads, n, t.max_slots, smem, grid, per_sm);              \
+        int rc = trace_grid<KIND, F, R>(E, t.threads, n, t.max_slots, img, smem, grid, per_sm);         \
         if (rc || !launch) return rc;                                                                   \
         return trace_launch<KIND, F, R>(t, *grid, *smem);                                               \
     }

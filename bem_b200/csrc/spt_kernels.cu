@@ -19,6 +19,7 @@
 #include <mutex>
 #include <stdarg.h>
 
+#include "spt_abi.hpp"
 #include "spt_device.cuh"
 
 namespace spt {
@@ -232,7 +233,7 @@ __global__ void assemble_kernel(const double* pr, const double* pz, int n, doubl
 // ===========================================================================
 // C ABI
 
-namespace {
+namespace spt_abi {
 thread_local char g_err[512];
 
 int fail(int code, const char* fmt, ...) {
@@ -247,6 +248,12 @@ int cuda_check(cudaError_t e, const char* what) {
     if (e != cudaSuccess) return fail(SPT_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
     return SPT_OK;
 }
+}  // namespace spt_abi
+
+namespace {
+using spt_abi::cuda_check;
+using spt_abi::fail;
+using spt_abi::g_err;
 
 int check_bem(const SptBem* b) {
     if (!b || !b->seg || !b->node) return fail(SPT_ERR_ARG, "BEM tables required for this geometry");
@@ -289,6 +296,25 @@ int check_bem(const SptBem* b) {
 }
 
 bool is_bem(int kind) { return kind == SPT_GEOM_TIP_BEM || kind == SPT_GEOM_WELL_BEM || kind == SPT_GEOM_POST_BEM; }
+
+// The BEM image-charge force of a tip or well geometry built with z0
+// (has_image): its tables must be given, with at most SPT_TRACE_IMAGE_MODES
+// modes (the per-mode arrays of the stage evaluation live in registers).
+int check_image(const SptGeometry* g, const SptBem* b, int max_group_size) {
+    if (!(g->kind == SPT_GEOM_TIP_BEM || g->kind == SPT_GEOM_WELL_BEM) || !g->has_image) return SPT_OK;
+    const SptImage& im = b->image;
+    if (im.n_nodes < 2 || !im.node || !im.seg || !im.quad || !im.a_inv)
+        return fail(SPT_ERR_ARG, "a BEM tip or well with an image plane (has_image) needs the image-charge tables");
+    if (im.n_max < 0 || im.n_max > SPT_TRACE_IMAGE_MODES)
+        return fail(SPT_ERR_CAPACITY, "image-charge n_max %d outside [0, %d] in the trace", im.n_max,
+                    SPT_TRACE_IMAGE_MODES);
+    if (im.n_quad <= 0 || im.n_quad % 4 || !(im.rho_floor > 0.0)) return fail(SPT_ERR_ARG, "bad image-charge tables");
+    if (!(g->z_handoff > 0.0)) return fail(SPT_ERR_ARG, "z_handoff must be > 0");
+    const int lim = im.mirror_symmetric ? 256 : 512;
+    if (max_group_size > lim)
+        return fail(SPT_ERR_CAPACITY, "groups with the BEM image force hold at most %d particles", lim);
+    return SPT_OK;
+}
 
 int check_surrogate_params(const SptTraceParams* p) {
     if (!p->sur_w || !p->sur_w16 || !p->sur_s_start || !p->sur_log_scale)
@@ -423,7 +449,8 @@ int spt_trace(const SptState* s, const SptTraceParams* p, const SptGeometry* g, 
     if (p->form != SPT_FORM_FP64 && p->form != SPT_FORM_MIXED && p->form != SPT_FORM_SURROGATE)
         return fail(SPT_ERR_ARG, "unknown form %d", p->form);
     if (is_bem(g->kind)) {
-        const int rc = check_bem(b);
+        int rc = check_bem(b);
+        if (!rc) rc = check_image(g, b, s->max_group_size);
         if (rc) return rc;
     }
     if (p->form == SPT_FORM_SURROGATE) {
@@ -441,7 +468,8 @@ int spt_accel(const SptAccelArgs* a, const SptGeometry* g, const SptBem* b, void
         return fail(SPT_ERR_CAPACITY, "spt_accel: group size must be in [1, %d]", spt::kSmallGroup);
     if (a->form != SPT_FORM_FP64 && a->form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "spt_accel: form %d", a->form);
     if (is_bem(g->kind)) {
-        const int rc = check_bem(b);
+        int rc = check_bem(b);
+        if (!rc) rc = check_image(g, b, a->max_group_size);
         if (rc) return rc;
     }
     SptBem bem = b ? *b : SptBem{};
@@ -639,7 +667,8 @@ extern "C" int spt_trace_noalloc(const SptState* s, const SptTraceParams* p, con
     if (p->form == SPT_FORM_SURROGATE) return fail(SPT_ERR_ARG, "spt_trace_noalloc: the learned form is not offered");
     if (p->form != SPT_FORM_FP64 && p->form != SPT_FORM_MIXED) return fail(SPT_ERR_ARG, "unknown form %d", p->form);
     if (is_bem(g->kind)) {
-        const int rc = check_bem(b);
+        int rc = check_bem(b);
+        if (!rc) rc = check_image(g, b, s->max_group_size);
         if (rc) return rc;
     }
     void* scratch = nullptr;

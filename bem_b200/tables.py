@@ -307,6 +307,15 @@ class BemTables:
             s.cluster_terms = CLUSTER_TERMS
             s.cluster_kappa = CLUSTER_KAPPA
 
+    def attach_image(self, solution):
+        """Add the image-charge tables of a geometry built with z0 (an
+        image_charge.ImageChargeSolution on the same device): every view then
+        carries them, and the trace adds the image force at every stage."""
+        if solution.n_max > _lib.TRACE_IMAGE_MODES:
+            raise ValueError(f"image_n_max {solution.n_max} above {_lib.TRACE_IMAGE_MODES} is not offered in the trace")
+        self.image = solution
+        self.struct.image = solution.struct
+
     def view(self, far_rule="reference", ratio4=RATIO4, ratio2=RATIO2, ratio_run=RATIO_RUN, bounds=True,
              cluster_kappa=None):
         """An SptBem over these tables with the given far rule (the tables

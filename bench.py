@@ -6,11 +6,14 @@ tracer's hot path on B200.
                     [--form mixed|fp64] [--far-rule adaptive|reference]
                     [--cta-threads 64|128|256] [--bins] [--no-tune] ...
 
-The chosen form (the default): float32 + Kahan BEM and pair sums (float64
-state, stage combination, error norm and controller, float64 for points
-close to a ring and for ill-conditioned sums) with the adaptive far-field
-rule, its launch configuration chosen first by the project's autotuner on a
-sample of the workload (untimed; `--no-tune` keeps the defaults).
+The chosen form (the default): float64 arithmetic with the adaptive
+far-field rule (the BEM far sum ~1e-14 from the reference's quadrature;
+the plain form's step sequence on ~99 % of groups), its launch
+configuration chosen first by the project's autotuner on a sample of the
+workload (untimed; `--no-tune` keeps the defaults).  `--form mixed` times
+the float32 + Kahan form instead; on the whole C1 trace it misses the 1e-6
+endpoint bar in a few groups, so the default run reports it beside the
+chosen form (accuracy.mixed_form) rather than as the headline.
 
 Workload (default c1, the largest single-GPU configuration with a BEM
 field): hemisphere R = 50 nm on a 5 um post, E = -1e6 V/m, 2000-panel BEM
@@ -498,10 +501,13 @@ def plain_and_accuracy(args, wl, pos, vel, tb, q, m, sizes, dev, t_max, budget):
     sub = (pos[:k], vel[:k], tb[:k], q[:k], m[:k], sizes[:n])
     out = {}
     stream = torch.cuda.current_stream(dev)
-    for name, form, rule in (("plain", "fp64", "reference"), ("chosen", args.form, args.far_rule)):
+    legs = [("plain", "fp64", "reference"), ("chosen", args.form, args.far_rule)]
+    if args.form == "fp64" and args.far_rule == "adaptive":
+        legs.append(("mixed", "mixed", "adaptive"))  # the float32 form, reported beside the chosen one
+    for name, form, rule in legs:
         tracer = make_tracer(args, wl, dev, form, rule)
         binned = False
-        if name == "chosen":
+        if name != "plain":
             binned = args.bins
             if getattr(args, "tuned_config", None):
                 from bem_b200 import autotune
@@ -526,6 +532,12 @@ def plain_and_accuracy(args, wl, pos, vel, tb, q, m, sizes, dev, t_max, budget):
                          vel=b.velocities().cpu().numpy(), td=b.t_death.cpu().numpy())
     P, C = out["plain"], out["chosen"]
     rate = lambda o: o["c"]["particle_steps"] / o["t"]
+
+    def errors(C):
+        d0, d1 = P["td"], C["td"]
+        alive = ~np.isfinite(d0) & ~np.isfinite(d1)
+        ex = np.linalg.norm(C["pos"] - P["pos"], axis=-1)[alive] / np.linalg.norm(P["pos"], axis=-1)[alive]
+        return ex
     span = f"whole trace to t = {t_max:.3g} s" if budget == WHOLE_TRACE else f"{budget} attempts from emission"
     plain = dict(value=rate(P), unit=UNIT, seconds=P["t"], form="fp64", far_rule="reference", groups=n,
                  chosen_value_same_groups=rate(C), chosen_seconds=C["t"], ratio=rate(C) / rate(P),
@@ -544,6 +556,14 @@ def plain_and_accuracy(args, wl, pos, vel, tb, q, m, sizes, dev, t_max, budget):
                max_rel_t_death=float(et.max()) if et.size else None,
                attempts_plain=int(P["c"]["attempts"]), attempts_chosen=int(C["c"]["attempts"]),
                accepted_steps_ratio=float(C["c"]["accepted"] / max(P["c"]["accepted"], 1)))
+    if "mixed" in out:
+        X = out["mixed"]
+        e = errors(X)
+        acc["mixed_form"] = dict(
+            note="float32 + Kahan pair and far sums, adaptive far rule: faster, but over 1e-6 on this span, so "
+                 "not the chosen form", value=rate(X), ratio_to_plain=rate(X) / rate(P),
+            max_rel_pos=float(e.max()) if e.size else None, particles_above_1e6=int((e > 1e-6).sum()),
+            accepted_steps_ratio=float(X["c"]["accepted"] / max(P["c"]["accepted"], 1)))
     return plain, acc
 
 
@@ -607,7 +627,8 @@ def main():
                     help="trace: a step is a whole trace from emission to t_end; slice: --attempts per group")
     ap.add_argument("--t-end", type=float, default=None, help="end of the trace span [s] (default per workload)")
     ap.add_argument("--attempts", type=int, default=16, help="--span slice: RK45 attempts per group per step")
-    ap.add_argument("--form", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"],
+                    help="arithmetic of the chosen form (fp64: the only form within 1e-6 on the whole C1 trace)")
     ap.add_argument("--far-rule", default="adaptive", choices=["reference", "adaptive"],
                     help="far-field quadrature of the BEM sum (adaptive: whole-segment Gauss-4/2 when distant)")
     ap.add_argument("--cta-threads", type=int, default=0, help="CTA width (0: autotuned, or the library's choice)")

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define SPT_ABI_VERSION 2
+#define SPT_ABI_VERSION 3
 
 /* return codes */
 #define SPT_OK 0
@@ -105,6 +105,27 @@ typedef struct {
  *   9 sigma0 (density at p0)  10 sigma1 (density at p1)              */
 #define SPT_SEG_FIELDS 11
 
+/* Largest azimuthal mode n_max the image-charge entry points accept. */
+#define SPT_IMAGE_MAX_MODES 64
+
+/* Tables of one image-charge solution (ImageChargeBEMSolution,
+ * bem/image_charge.py:457-620), built once per geometry by the host. */
+typedef struct {
+    int32_t n_nodes;          /* P profile nodes (at least 2) */
+    int32_t n_max;            /* modes 0..n_max, at most SPT_IMAGE_MAX_MODES */
+    int32_t n_quad;           /* reconstruction nodes: (P-1) * n_subdiv * 4 */
+    int32_t mirror_symmetric; /* profile mirror-doubled through z = -z0 (image_mirror_symmetric=True):
+                                 phantom sources (z -> -2 z0 - z, -q) join the solve, the plane image is
+                                 added back, and a source whose plane is nearer than the profile takes
+                                 no local mirror charge (bem/geometry.py:346-415, image_charge.py:538-585) */
+    const double* node;       /* [2][P]: rho (floored at rho_floor), z of the profile nodes */
+    const double* seg;        /* [6][P-1]: p0_rho p0_z tan_rho tan_z normal_rho normal_z (tan = p1 - p0) */
+    const double* quad;       /* [5][n_quad]: rho z length-weight t segment-index (image_charge.py:418-452) */
+    const double* a_inv;      /* [(n_max+1) x P x P] row-major: the inverse of each mode's operator */
+    double rho_floor;         /* 1e-6 * max profile rho */
+    double d_lo, d_hi;        /* mirror-charge blend distances [m] (image_charge_weight; d_hi <= d_lo: no mirror) */
+} SptImage;
+
 /* Precomputed BEM solution tables (bem/axisymmetric.py:305-338, 490-498).
  * `node` holds 3 rows of node_stride doubles: rho_q, z_q, w_q = area_q*sigma_q
  * for the n_seg*nodes_per_seg Gauss-4 far-quadrature nodes, segment-major.
@@ -169,7 +190,16 @@ typedef struct {
     int32_t cluster_levels;
     int32_t cluster_terms;
     double cluster_kappa;
+    /* BEM image-charge force (geometries built with z0: kind SPT_GEOM_TIP_BEM
+     * or SPT_GEOM_WELL_BEM with has_image): the tables of the image profile's
+     * mode solve.  spt_trace and spt_accel add the geometry-level force of
+     * spt_image_force to every stage (n_max at most SPT_TRACE_IMAGE_MODES
+     * there); n_nodes = 0: none. */
+    SptImage image;
 } SptBem;
+
+/* Largest image-charge n_max inside spt_trace / spt_accel. */
+#define SPT_TRACE_IMAGE_MODES 16
 
 #define SPT_MAX_CLUSTER_RUNS 256
 
@@ -355,6 +385,49 @@ int spt_ellip_ke(const double* p, int64_t n, int32_t form, double* K, double* E,
  * 4) on each leaf.  profile_rho/z are [n_nodes] device arrays. */
 int spt_bem_assemble(const double* profile_rho, const double* profile_z, int32_t n_nodes, double refine_ratio,
                      int32_t max_depth, const double* gauss4_x, const double* gauss4_w, double* A, void* stream);
+
+/* ---- BEM image-charge force (azimuthal Fourier modes) ------------------
+ * The induced-charge force of an axisymmetric grounded conductor on the
+ * particles of each group (bem/image_charge.py, bem/ring_modes.py,
+ * bem/toroidal.py; used by bem/geometry.py:326-344, 780-797 when a BEM
+ * geometry is built with z0). */
+
+
+/* Toroidal harmonics Q_{m-1/2}(chi) and dQ_{m-1/2}/dchi, m = 0..n_max, for
+ * chi >= 1 (clipped to the next double above 1): q, dq are [(n_max+1) x n]
+ * row-major.  Replaces toroidal_Q, bem/toroidal.py:180-219. */
+int spt_toroidal_q(const double* chi, int64_t n, int32_t n_max, double* q, double* dq, void* stream);
+
+/* Per-mode single-layer collocation operators of a generating profile:
+ * A [(n_max+1) x n_nodes x n_nodes] row-major, A[m][i][j] = mode-m
+ * potential at node i (rho floored at rho_floor, which the reference sets
+ * to 1e-6 max rho) of the unit hat density
+ * of node j, by the adaptive bisection of spt_bem_assemble with the mode
+ * kernel Phi_m on each Gauss-4 leaf.  Replaces assemble_mode_operators,
+ * bem/image_charge.py:379-411, 470-495. */
+int spt_image_assemble(const double* profile_rho, const double* profile_z, int32_t n_nodes, int32_t n_max,
+                       double rho_floor, double refine_ratio, int32_t max_depth, const double* gauss4_x,
+                       const double* gauss4_w, double* A, void* stream);
+
+
+/* Image-charge force on the particles of every group, [n_particles]:
+ * the joint per-group solve of ImageChargeBEMSolution.image_force
+ * (bem/image_charge.py:816-1056) -- local mirror charges, per-mode RHS,
+ * sigma = A^-1 rhs, field on the fixed quadrature, direct mirror field.
+ * With geom == NULL that solution-level force alone (in N); with a geometry
+ * (kind SPT_GEOM_TIP_BEM or SPT_GEOM_WELL_BEM, has_image set) the
+ * geometry's image_force: the flat plane image at geom->z0 above
+ * geom->z_handoff, the BEM image force below z_handoff / 2, smoothstep
+ * between (plummer_radius softens the plane image).  Inactive particles
+ * (active[i] == 0) neither excite the solve nor feel a force.  At most 512
+ * particles per group (256 with mirror_symmetric).  Shared memory per CTA:
+ * 8 * (10 S + 3 E + 2 (1 + c) (n_max+1) n_nodes) bytes, S = E (2E with
+ * mirror_symmetric) sources, c in [1, 8] partial right-hand sides; it must
+ * fit 227 KB with c = 1 (SPT_ERR_CAPACITY otherwise). */
+int spt_image_force(const double* x, const double* y, const double* z, const double* charge, const uint8_t* active,
+                    const int64_t* group_offset, int32_t n_groups, int32_t max_group_size, const SptImage* image,
+                    const SptGeometry* geom, double coulomb_constant, double plummer_radius, double* fx, double* fy,
+                    double* fz, void* stream);
 
 /* spt_trace for callers that cannot allocate device memory: a caller with no
  * device allocator of its own (a cgo/JNI/ctypes binding without torch), or

@@ -7,8 +7,11 @@ A *spec* is a plain dict (``kind`` plus parameters; BEM kinds also carry
 
 * ``flat``     -- geometry.FlatCathode
 * ``tip``      -- geometry.HemisphericalTip (analytic field, 3-image force)
-* ``tip_bem``  -- bem.geometry.HemisphericalTipBEMGeometry with z0=None
-* ``well_bem`` -- bem.geometry.CylindricalWellBEMGeometry with z0=None
+* ``tip_bem``  -- bem.geometry.HemisphericalTipBEMGeometry; with ``z0`` the
+  spec also carries ``image_profile``, ``image_n_max``, ``image_d_lo``,
+  ``image_d_hi``, ``image_mirror_symmetric`` (optional ``image_A``) for the
+  BEM image-charge force
+* ``well_bem`` -- bem.geometry.CylindricalWellBEMGeometry (the same image keys)
 * ``post_bem`` -- hemisphere of radius R on a cylindrical post of height L:
   BEM field of the mirror-doubled capsule blended with the flat fallback,
   and the 3-image force of forces.hemispherical_tip_image_force applied in
@@ -73,7 +76,17 @@ def image_force(spec, pos, q, live, soft):
         shifted = pos.copy()
         shifted[..., 2] = pos[..., 2] - spec["L"]
         return _ph.tip_images(shifted, q, live, spec["R"] - z0, soft, plane_z0=spec["L"] + z0)
-    raise ValueError(f"image force of kind {k!r} with z0 set is the BEM image solve (not on this path)")
+    if k in ("tip_bem", "well_bem"):
+        # bem/geometry.py:326-344, 780-797: the BEM image-charge solve (oracle/image_charge.py)
+        from . import image_charge as _ic
+        sol = spec.get("_image_oracle")
+        if sol is None:
+            sol = _ic.ImageSolution(spec["image_profile"], spec["image_n_max"], A=spec.get("image_A"))
+            spec["_image_oracle"] = sol
+        return _ic.geometry_image_force(sol, pos, q, live, z0, spec["R"], spec["image_d_lo"], spec["image_d_hi"],
+                                        z_handoff=spec["z_handoff"],
+                                        mirror_symmetric=spec.get("image_mirror_symmetric", False), soft=soft)
+    raise ValueError(f"unknown geometry kind {k!r}")
 
 
 def kill_mask(spec, pos, z_max=None):

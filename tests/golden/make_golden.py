@@ -303,6 +303,40 @@ def gen_trace_well():
           n_subdiv=8, **res)
 
 
+def gen_trace_image():
+    """Traces with the BEM image-charge force: HemisphericalTipBEMGeometry
+    (R = 50 nm, z0 = 3 nm; the truncated-plane image surface and the
+    mirror-doubled one) and CylindricalWellBEMGeometry (R = 200 nm,
+    H = 100 nm, z0 = 3 nm), 2 groups of 4 electrons each, emitted 1 nm off
+    the real surface, through the reference's integrate to a short t_max."""
+    from specific_particle_tracer.bem.geometry import CylindricalWellBEMGeometry, HemisphericalTipBEMGeometry
+    from specific_particle_tracer.constants import ev_to_kg
+    from bem_b200 import workloads as w
+    m = ev_to_kg(510998.95069)
+    R, z0 = 50e-9, 3e-9
+    for tag, sym in (("trunc", False), ("doubled", True)):
+        geo = HemisphericalTipBEMGeometry(-1e8, R, field_max_length=R * np.pi / 30, z0=z0, image_mirror_symmetric=sym)
+        d = w.tip_c2(n_groups=2, n_emit=4, R=R, L=0.0, seed=25, t_spread=0.1e-12)
+        pos, vel, tb = _grouped(d, 2, 4, m)
+        pos = pos * (1.0 + 1e-9 / R)  # 1 nm off the sphere along its normal
+        res = _trace_groups(geo, pos, vel, tb, 0.25e-12, 1e-8, 1e-12, 3e-7, procs=2)
+        sol, img = geo.field_solver.solution, geo.image_solution
+        _save(f"trace_image_tip_{tag}", profile=sol.profile, sigma=sol.sigma, R=R, E_gun=-1e8, z0=z0,
+              z_handoff=geo.z_handoff, n_subdiv=8, image_profile=img.profile, image_n_max=geo.image_n_max, image_d_lo=geo.image_d_lo, image_d_hi=geo.image_d_hi,
+              image_mirror_symmetric=sym, **res)
+    R, H = 200e-9, 100e-9
+    geo = CylindricalWellBEMGeometry(-1e8, R, H, field_max_length=H / 8, z0=z0)
+    d = w.well_c3(n_groups=8, seed=26, R=R, H=H, t_spread=0.1e-12)
+    pos, vel, tb = _grouped(d, 2, 4, m)
+    pos = pos + np.array([0.0, 0.0, 1e-9])
+    res = _trace_groups(geo, pos, vel, tb, 0.25e-12, 1e-8, 1e-12, 3e-6, procs=2)
+    sol, img = geo.field_solver.solution, geo.image_solution
+    _save("trace_image_well", profile=sol.profile, sigma=sol.sigma, R=R, H=H, E_gun=-1e8, z0=z0,
+          z_handoff=geo.z_handoff, n_subdiv=8, bottom_fillet_radius=geo.bottom_fillet_radius,
+          rim_fillet_radius=geo.rim_fillet_radius, image_profile=img.profile, image_n_max=geo.image_n_max, image_d_lo=geo.image_d_lo, image_d_hi=geo.image_d_hi,
+          image_mirror_symmetric=False, **res)
+
+
 def gen_tracker():
     """Tracker-level outputs (screens, t_out) for a small flat case."""
     from specific_particle_tracer import SpecificParticleTracer, geometry as g
@@ -500,9 +534,12 @@ def gen_trace_c4(bins=C4_BINS):
 def gen_trace_c3(bins=C3_BINS):
     """C3 size bins on the reference's own ~3000-segment well (R = 2 um,
     H = 1 um, E = -2.5e6 V/m, max_length H/980): the C3 sampler (seed 3,
-    fixed sizes), 8 groups of 1 and 4 of 2 traced to t = 30 ps, one group
-    each of 129 and 256 for 60 attempts (their sites lifted 1 nm off the
-    floor, for the reason of _lift_cap)."""
+    fixed sizes), 8 groups of 1 and 4 of 2 traced to t = 30 ps (with two
+    more reference runs at vel0 x (1 -+ 1e-15) that record its own
+    sensitivity), one group each of 129 and 256 for 60 attempts; every site
+    lifted 1 nm off the floor (for the reason of _lift_cap: on the floor itself a point sits on
+    the on-surface offset threshold, which moves the early step sizes and
+    with them the death time of a particle that returns to the floor)."""
     from specific_particle_tracer.bem.geometry import CylindricalWellBEMGeometry
     from bem_b200 import workloads as w
     R, H = 2e-6, 1e-6
@@ -514,24 +551,110 @@ def gen_trace_c3(bins=C3_BINS):
     for E, n, att in bins:
         d = w.well_c3(seed=3, sizes=[E] * n)
         pos, vel, tb = _bench_groups(d, 0, n, E)
-        if att:
-            pos = pos + np.array([0.0, 0.0, 1e-9])
+        pos = pos + np.array([0.0, 0.0, 1e-9])
         res = _trace_groups(geo, pos, vel, tb, 30e-12, 1e-9, 1e-12, 2e-3, max_attempts=att)
+        if not att:
+            # the reference's own sensitivity: the same groups with vel0 scaled by 1 -+ 1e-15 (a group whose
+            # attempt sequence changes under it returns to the floor, where the decisions are ill-conditioned)
+            pert = [_trace_groups(geo, pos, vel * (1.0 + e), tb, 30e-12, 1e-9, 1e-12, 2e-3) for e in (1e-15, -1e-15)]
+            res.update(attempts_pert=np.stack([r["attempts"] for r in pert]),
+                       t_death_pert=np.stack([r["t_death"] for r in pert]),
+                       pos_pert=np.stack([r["pos"] for r in pert]), vel_pert=np.stack([r["vel"] for r in pert]))
         _save(f"trace_c3_s{E}", profile=sol.profile, sigma=sol.sigma, R=R, H=H, E_gun=-2.5e6,
               z_handoff=geo.z_handoff, n_subdiv=8, **res)
 
 
-GENERATORS = dict(sigma_c1=gen_sigma_c1, ellip=gen_ellip, ring=gen_ring, accel=gen_accel, bem_sphere=gen_bem_sphere,
+def gen_toroidal():
+    """Q_{m-1/2}, dQ/dchi (both recurrence branches, near coincidence to far)
+    and the mode kernels on random (field, source) pairs."""
+    from specific_particle_tracer.bem.ring_modes import point_charge_potential_modes, ring_field_modes
+    from specific_particle_tracer.bem.toroidal import toroidal_Q
+    rng = np.random.default_rng(21)
+    chi = np.concatenate([1.0 + np.logspace(-14, 3, 300), [1.0, np.nextafter(1.0, 2.0), 1.0 + 1e-300]])
+    q, dq = toroidal_Q(chi, 24)
+    n = 400
+    a = rng.uniform(1e-9, 1e-7, n)
+    za = rng.normal(0.0, 5e-8, n)
+    rho = a * np.exp(rng.uniform(-4.0, 3.0, n))
+    z = za + a * rng.normal(0.0, 1.0, n) * np.exp(rng.uniform(-6.0, 1.0, n))
+    ph, dr, dz = ring_field_modes(rho, z, a, za, 16)
+    g = point_charge_potential_modes(rho, z, a, za, 16)
+    _save("toroidal", chi=chi, q=q, dq=dq, rho=rho, z=z, a=a, za=za, phi_m=ph, dphi_drho=dr, dphi_dz=dz, g=g)
+
+
+def _image_states(rng, G, E, R, lift_lo, lift_hi, theta_max):
+    """Points above the real hemisphere-on-plane surface: lifted off the cap
+    by lift in [lift_lo, lift_hi] at polar angles below theta_max, random
+    azimuths; a fifth of them inactive."""
+    th = rng.uniform(0.0, theta_max, (G, E))
+    ph = rng.uniform(-np.pi, np.pi, (G, E))
+    r = R + rng.uniform(lift_lo, lift_hi, (G, E))
+    pos = np.stack([r * np.sin(th) * np.cos(ph), r * np.sin(th) * np.sin(ph), r * np.cos(th)], -1)
+    active = rng.uniform(0.0, 1.0, (G, E)) > 0.2
+    q = np.full((G, E), -1.602176634e-19) * rng.uniform(0.5, 2.0, (G, E))
+    return pos, q, active
+
+
+def gen_image_tip():
+    """The BEM image-charge force on the hemisphere-on-plane tip (R = 50 nm,
+    z0 = 3 nm): the truncated-plane image profile (operators, per-call
+    ImageChargeBEMSolution.image_force) and the geometry-level force of
+    HemisphericalTipBEMGeometry(z0=3 nm) in both image modes."""
+    from specific_particle_tracer.bem.geometry import HemisphericalTipBEMGeometry
+    R, z0 = 50e-9, 3e-9
+    rng = np.random.default_rng(22)
+    out = {}
+    pos, q, active = _image_states(rng, 3, 5, R, 1e-9, 4e-8, np.radians(60.0))
+    pos[2, :, :] = pos[0, :, :]  # group 2 = group 0 with other charges: groups are independent
+    out.update(pos=pos, q=q, active=active, R=R, z0=z0, d_lo=0.1, d_hi=0.5)
+    for tag, sym in (("trunc", False), ("doubled", True)):
+        geo = HemisphericalTipBEMGeometry(-1e8, R, z0=z0, image_mirror_symmetric=sym)
+        sol = geo.image_solution
+        out[f"{tag}_profile"] = sol.profile
+        out[f"{tag}_A"] = sol.A
+        out[f"{tag}_n_max"] = sol.n_max
+        out[f"{tag}_z_handoff"] = geo.z_handoff
+        out[f"{tag}_force"] = geo.image_force(pos, q, active, 1e-12)
+        if not sym:
+            out["trunc_solution_force"] = sol.image_force(pos, q, active, 0.1 * R, 0.5 * R, n_max=sol.n_max)
+            out["trunc_solution_force_nomirror"] = sol.image_force(pos, q, active, 0.1 * R, 0.1 * R,
+                                                                   n_max=sol.n_max)
+    _save("image_tip", **out)
+
+
+def gen_image_well():
+    """CylindricalWellBEMGeometry(z0=3 nm) on a small well (R = 200 nm,
+    H = 100 nm): its image profile's operators and the geometry-level image
+    force at points inside and above the recess."""
+    from specific_particle_tracer.bem.geometry import CylindricalWellBEMGeometry
+    R, H, z0 = 200e-9, 100e-9, 3e-9
+    rng = np.random.default_rng(23)
+    geo = CylindricalWellBEMGeometry(-1e7, R, H, z0=z0)
+    sol = geo.image_solution
+    G, E = 3, 4
+    rho = R * np.sqrt(rng.uniform(0.0, 0.8, (G, E)))
+    ph = rng.uniform(-np.pi, np.pi, (G, E))
+    z = rng.uniform(-H + 5e-9, 60e-9, (G, E))
+    pos = np.stack([rho * np.cos(ph), rho * np.sin(ph), z], -1)
+    active = rng.uniform(0.0, 1.0, (G, E)) > 0.2
+    q = np.full((G, E), -1.602176634e-19)
+    force = geo.image_force(pos, q, active, 1e-12)
+    _save("image_well", profile=sol.profile, A=sol.A, n_max=sol.n_max, z_handoff=geo.z_handoff, R=R, H=H, z0=z0,
+          d_lo=geo.image_d_lo, d_hi=geo.image_d_hi, pos=pos, q=q, active=active, force=force)
+
+
+GENERATORS = dict(sigma_c1=gen_sigma_c1, toroidal=gen_toroidal, image_tip=gen_image_tip, image_well=gen_image_well, ellip=gen_ellip, ring=gen_ring, accel=gen_accel, bem_sphere=gen_bem_sphere,
                   bem_well=gen_bem_well, bem_post=gen_bem_post, trace_flat=gen_trace_flat,
                   trace_tip=gen_trace_tip, trace_tip_bem=gen_trace_bem, trace_post=gen_trace_post,
                   trace_well=gen_trace_well, tracker=gen_tracker,
                   trace_flat_c0=lambda: gen_trace_flat(16), trace_c1=gen_trace_c1, trace_c2=gen_trace_c2,
                   trace_c3=gen_trace_c3, trace_c4=gen_trace_c4,
-                  trace_c3_budget=lambda: gen_trace_c3(C3_BINS[2:]), trace_c4_budget=lambda: gen_trace_c4(C4_BINS[3:]))
+                  trace_c3_budget=lambda: gen_trace_c3(C3_BINS[2:]), trace_c4_budget=lambda: gen_trace_c4(C4_BINS[3:]),
+                  trace_c3_small=lambda: gen_trace_c3(C3_BINS[:2]), trace_image=gen_trace_image)
 
 # generated only when named (minutes to an hour of CPU each)
 ON_REQUEST = ("trace_flat_c0", "sigma_c1", "trace_c1", "trace_c2", "trace_c3", "trace_c4", "trace_c3_budget",
-              "trace_c4_budget")
+              "trace_c4_budget", "trace_c3_small", "trace_image")
 
 
 def main():

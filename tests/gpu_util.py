@@ -19,15 +19,22 @@ def device_geometry(spec):
         return bg.FlatCathode(spec["E_gun"], z0=spec.get("z0"), kill_z_below=spec.get("kill_z_below", 0.0))
     if k == "tip":
         return bg.HemisphericalTip(spec["E_gun"], spec["R"], z0=spec.get("z0"), kill_z_below=spec.get("kill_z_below", 0.0))
+    img = {}
+    if spec.get("z0") is not None and k in ("tip_bem", "well_bem"):  # the BEM image-charge force
+        img = dict(z0=spec["z0"], image_n_max=spec["image_n_max"], image_d_lo=spec["image_d_lo"],
+                   image_d_hi=spec["image_d_hi"], image_profile=spec["image_profile"])
+        if k == "tip_bem":
+            img["image_mirror_symmetric"] = spec.get("image_mirror_symmetric", False)
     if k == "tip_bem":
         return bg.HemisphericalTipBEMGeometry(spec["E_gun"], spec["R"], n_subdiv=spec["n_subdiv"],
                                               z_handoff=spec["z_handoff"], kill_z_below=spec.get("kill_z_below", 0.0),
-                                              profile=spec["profile"], sigma=spec["sigma"])
+                                              profile=spec["profile"], sigma=spec["sigma"], **img)
     if k == "well_bem":
         return bg.CylindricalWellBEMGeometry(spec["E_gun"], spec["R"], spec["H"], n_subdiv=spec["n_subdiv"],
                                              bottom_fillet_radius=spec.get("bottom_fillet_radius"),
                                              rim_fillet_radius=spec.get("rim_fillet_radius"),
-                                             z_handoff=spec["z_handoff"], profile=spec["profile"], sigma=spec["sigma"])
+                                             z_handoff=spec["z_handoff"], profile=spec["profile"], sigma=spec["sigma"],
+                                             **img)
     if k == "post_bem":
         return bg.PostTipBEMGeometry(spec["E_gun"], spec["R"], spec["L"], n_subdiv=spec["n_subdiv"], z0=spec.get("z0"),
                                      z_handoff=spec["z_handoff"], kill_z_below=spec.get("kill_z_below", 0.0),

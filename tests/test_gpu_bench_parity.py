@@ -65,6 +65,10 @@ def _run(spec, fixtures, form, budget_first=None, binned=False):
     f0 = fixtures[0]
     t_max, rtol, atol, z_max = float(f0["t_max"]), float(f0["rtol"]), float(f0["atol"]), float(f0["z_max"])
     n = len(pos)
+    if budget_first is None:  # fixtures the reference cut after a fixed number of attempts
+        budgets = {int(f["max_attempts"]) for f in fixtures if int(f["max_attempts"]) > 0}
+        assert len(budgets) <= 1
+        budget_first = budgets.pop() if budgets else None
     tr = engine.Tracer(gu.device_geometry(spec), form=form[0], far_rule=form[1], z_max=z_max)
     batch = engine.GroupBatch(pos, vel, tb, np.full(n, gu.Q_E), np.full(n, gu.M_E), sizes)
     snaps = {}
@@ -118,23 +122,44 @@ def _check(f, o, form):
     dead = np.isfinite(f["t_death"]) & np.isfinite(o["t_death"])
     # every particle killed in one run is killed in the other
     np.testing.assert_array_equal(np.isfinite(o["t_death"]), np.isfinite(f["t_death"]))
+    # groups whose attempt sequence the reference itself changes when vel0 moves by 1e-15 (recorded in
+    # the fixture): their decisions are ill-conditioned, so they are compared by the reference's own spread
+    ill = np.zeros(len(f["attempts"]), dtype=bool)
+    spread = np.zeros_like(f["t_death"])
+    if "attempts_pert" in f:
+        ill = np.any(f["attempts_pert"] != f["attempts"][None], axis=0)
+        with np.errstate(invalid="ignore"):
+            spread = np.nan_to_num(np.max(np.abs(f["t_death_pert"] - f["t_death"][None]), axis=0) / f["t_death"])
     if form == PLAIN:
         same = (o["attempts"] == f["attempts"]) & (o["n_acc"] == f["n_acc"])
-        assert same.mean() >= 0.99, (o["attempts"], f["attempts"], o["n_acc"], f["n_acc"])
+        assert same[~ill].mean() >= 0.99, (o["attempts"], f["attempts"], o["n_acc"], f["n_acc"])
         # groups with no kill: 1e-10 relative on positions and velocities
-        clean = ~np.any(np.isfinite(f["t_death"]), axis=1)
+        clean = ~np.any(np.isfinite(f["t_death"]), axis=1) & ~ill
         if clean.any():
             assert _rel(o["pos"][clean], f["pos"][clean]).max() < 1e-10
             assert _rel(o["vel"][clean], f["vel"][clean]).max() < 1e-10
-        np.testing.assert_allclose(o["t"], f["t"], rtol=1e-12)
+        # group times are sums of the accepted step sizes, which carry the
+        # error norm's cancellation (ulp-level slope differences become ~1e-12
+        # of t after a hundred steps): compared at the endpoint bound
+        np.testing.assert_allclose(o["t"][~ill], f["t"][~ill], rtol=1e-10)
         tol = 1e-10
     else:
         tol = 1e-6
     if alive.any():
-        assert _rel(o["pos"][alive], f["pos"][alive]).max() < tol
-        assert _rel(o["vel"][alive], f["vel"][alive]).max() < tol
+        ok = alive & ~ill[:, None]
+        if ok.any():
+            assert _rel(o["pos"][ok], f["pos"][ok]).max() < tol
+            assert _rel(o["vel"][ok], f["vel"][ok]).max() < tol
+        if "pos_pert" in f and (alive & ill[:, None]).any():
+            loose = alive & ill[:, None]
+            for key in ("pos", "vel"):
+                ref_spread = max(_rel(p[loose], f[key][loose]).max() for p in f[key + "_pert"])
+                assert _rel(o[key][loose], f[key][loose]).max() <= max(tol, 10.0 * ref_spread)
     if dead.any():
-        np.testing.assert_allclose(o["t_death"][dead], f["t_death"][dead], rtol=max(tol, 1e-7))
+        # death times move with the step grid (~1e-7 of a step, the error norm's cancellation), and by the
+        # reference's own spread where its decisions are ill-conditioned
+        rt = np.maximum(max(tol, 1e-7), 10.0 * spread[dead])
+        assert np.all(np.abs(o["t_death"][dead] - f["t_death"][dead]) <= rt * np.abs(f["t_death"][dead]))
 
 
 @pytest.mark.parametrize("form", [PLAIN, CHOSEN], ids=["plain", "chosen"])
