@@ -11,10 +11,14 @@ The knobs change speed, not physics:
   point; more points share node loads and the adaptive rule's
   classification.  Results agree to rounding.
 * ``ratios`` -- thresholds (ratio4, ratio2, ratio_run) of the adaptive far
-  rule.  Candidates pass an accuracy guard first: at the sample's own
-  trajectory points their float64 field must match the reference quadrature
-  to ``tol`` of the whole field (uniform plus perturbation); a candidate that
-  does not is never timed.
+  rule, tuned only with ``tune_ratios=True``.  Candidates pass an accuracy
+  guard first: at the sample's own trajectory points their float64 field
+  must match the reference quadrature to ``tol`` of the whole field; a
+  candidate that does not is never timed.  The guard is necessary, not
+  sufficient: on the whole C1 trace the (6, 150, 3) thresholds passed it and
+  still moved one group's endpoints by 2.6e-5 from the plain form (the
+  defaults: 2e-7), so by default the thresholds stay the defaults, whose
+  endpoint error is measured on whole traces.
 
 The group processing order is not tuned: it sets the load balance of the
 tail of the full grid, which a sample of groups cannot measure, so it stays
@@ -88,8 +92,9 @@ def _accuracy_ok(tracer, pos, ratios, tol):
 
 
 def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plummer_radius, charge_to_mass,
-         n_sample=2368, warm=200, attempts=32, repeats=3, tol=1e-11, margin=0.03, cache=None, threads=CTA_THREADS):
-    """Choose the CTA width, round_points and the adaptive rule's ratios for `tracer` on
+         n_sample=2368, warm=200, attempts=32, repeats=3, tol=1e-11, margin=0.03, cache=None, threads=CTA_THREADS,
+         tune_ratios=False):
+    """Choose the CTA width, round_points (and with tune_ratios the adaptive rule's ratios) for `tracer` on
     this workload (arrays as for GroupBatch; the order stays largest first).  Returns a
     TuneResult; `apply` sets it.  `cache`: a JSON file path (read if it holds
     this signature, updated otherwise)."""
@@ -149,7 +154,7 @@ def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plum
         for rp in ROUND_POINTS:
             rates[rp] = timings[f"round_points={rp}"] = timed(cfg["order"], rp, cfg["ratios"], cfg["cta_threads"])
         cfg["round_points"] = pick(rates, 4)
-        if tracer.tables is not None and tracer.far_rule == "adaptive":
+        if tune_ratios and tracer.tables is not None and tracer.far_rule == "adaptive":
             sample_pos = base.positions().cpu().numpy()
             rates = {}
             for r in RATIOS:

@@ -550,7 +550,7 @@ __device__ void far_round(Ctx& c, int r0, int np_, int n_tiles, int segs_per_til
                                 } else {
                                     // close to the ring: the term in float64, summed like the others
                                     double e64r, e64z;
-                                    ring_field_far(pr[p], 1.0 / pr[p], dz, rq[j], e64r, e64z);
+                                    ring_field_far_cold(pr[p], 1.0 / pr[p], dz, rq[j], e64r, e64z);
                                     const float ter = (float)(wq[j] * e64r), tez = (float)(wq[j] * e64z);
                                     kahan_add(fr[p], kr[p], ter);
                                     kahan_add(fz[p], kz[p], tez);
@@ -852,7 +852,7 @@ __device__ bool far_adaptive_warp(Ctx& c, int r0, int np_, unsigned long long& f
                             } else {
                                 // close to the ring: the term in float64, summed like the others
                                 double e64r, e64z;
-                                ring_field_far(pr[p], 1.0 / pr[p], dz, rq[j], e64r, e64z);
+                                ring_field_far_cold(pr[p], 1.0 / pr[p], dz, rq[j], e64r, e64z);
                                 const float ter = (float)(wq[j] * e64r), tez = (float)(wq[j] * e64z);
                                 kahan_add(fr[p], kr[p], ter);
                                 kahan_add(fz[p], kz[p], tez);
@@ -1054,10 +1054,18 @@ __device__ __forceinline__ void near_point(Ctx& c, int k, unsigned long long& n_
 // Adaptive far rule for record k, by this warp: float32 first in the mixed
 // form, float64 again when its sum is ill-conditioned.  The float64 tile is
 // the float64 form's, so with every sum redone the mixed form reproduces it.
+// Ring evaluations each lane keeps in flight in the float64 adaptive far sum.
+// Four, not eight: every in-flight evaluation is an inlined copy of the ring
+// kernel, and the trace kernel is bound by instruction fetch (measured: the
+// whole C1 trace 1.38x faster at four).
+#ifndef SPT_FAR_NQ_FP64
+#define SPT_FAR_NQ_FP64 4
+#endif
+
 template <int FORM>
 __device__ __forceinline__ void far_point(Ctx& c, int k, unsigned long long& fe, unsigned long long& ce) {
     if constexpr (FORM == SPT_FORM_FP64) {
-        far_adaptive_warp<1, 8, false>(c, k, 1, fe, ce);
+        far_adaptive_warp<1, SPT_FAR_NQ_FP64, false>(c, k, 1, fe, ce);
     } else {
         // float32 tiles keep 4 ring evaluations in flight per lane (8 spill at
         // 128 registers; more resident warps supply the parallelism instead)
@@ -2043,56 +2051,58 @@ trace_kernel(const __grid_constant__ SptState st, const __grid_constant__ SptTra
             const double t = gs.t, hr = gs.hr;
             for (int i = tid; i < E; i += nt) c.live[i] = (t >= c.tb[i]) && (t < c.td[i]);
             __syncthreads();
-            for (int s = 0; s < 6; ++s) {
+            // seven stage evaluations through one call site of stage_accel (a second
+            // inlined copy of the stage code would double the kernel's instruction footprint)
+            for (int s = 0; s < 7; ++s) {
                 double* const kps = KP(s);
-                for (int i = tid; i < E; i += nt) {
-                    double p[6];
+                if (s < 6) {
+                    for (int i = tid; i < E; i += nt) {
+                        double p[6];
 #pragma unroll
-                    for (int k = 0; k < 6; ++k) p[k] = Y0[k * Emax + i];
-                    for (int j = 0; j < s; ++j) {
-                        const double a = kA[s][j];
-                        if (a == 0.0) continue;
-                        const double ha = __dmul_rn(hr, a);
-                        const double* kpj = KP(j);
-                        const double* kvj = KV(j);
+                        for (int k = 0; k < 6; ++k) p[k] = Y0[k * Emax + i];
+                        for (int j = 0; j < s; ++j) {
+                            const double a = kA[s][j];
+                            if (a == 0.0) continue;
+                            const double ha = __dmul_rn(hr, a);
+                            const double* kpj = KP(j);
+                            const double* kvj = KV(j);
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                p[k] = __dadd_rn(p[k], __dmul_rn(ha, kpj[k * E + i]));
+                                p[3 + k] = __dadd_rn(p[3 + k], __dmul_rn(ha, kvj[k * E + i]));
+                            }
+                        }
+                        const bool lv = c.live[i];
 #pragma unroll
                         for (int k = 0; k < 3; ++k) {
-                            p[k] = __dadd_rn(p[k], __dmul_rn(ha, kpj[k * E + i]));
-                            p[3 + k] = __dadd_rn(p[3 + k], __dmul_rn(ha, kvj[k * E + i]));
+                            c.sp[k * E + i] = p[k];
+                            kps[k * E + i] = lv ? p[3 + k] : 0.0;
                         }
                     }
-                    const bool lv = c.live[i];
+                } else {
+                    // 5th-order solution and the endpoint stage (batched_rk45.py:365-370)
+                    for (int i = tid; i < E; i += nt) {
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        c.sp[k * E + i] = p[k];
-                        kps[k * E + i] = lv ? p[3 + k] : 0.0;
+                        for (int k = 0; k < 3; ++k) {
+                            double sp = 0.0, sv = 0.0;
+#pragma unroll
+                            for (int j = 0; j < 6; ++j) {
+                                sp = __dadd_rn(sp, __dmul_rn(kB[j], KP(j)[k * E + i]));
+                                sv = __dadd_rn(sv, __dmul_rn(kB[j], KV(j)[k * E + i]));
+                            }
+                            const double pn = __dadd_rn(Y0[k * Emax + i], __dmul_rn(hr, sp));
+                            const double vn = __dadd_rn(Y0[(3 + k) * Emax + i], __dmul_rn(hr, sv));
+                            NW[k * Emax + i] = pn;
+                            NW[(3 + k) * Emax + i] = vn;
+                            c.sp[k * E + i] = pn;
+                            kps[k * E + i] = c.live[i] ? vn : 0.0;
+                        }
                     }
                 }
                 __syncthreads();
                 c.key = (uint32_t)g * 2654435761u ^ (uint32_t)(gs.n_acc + gs.n_rej) * 40503u ^ (uint32_t)s * 97u;
                 stage_accel<KIND, FORM, FAR>(c, KV(s), &s_flag);
             }
-            // 5th-order solution and the endpoint stage (batched_rk45.py:365-370)
-            for (int i = tid; i < E; i += nt) {
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    double sp = 0.0, sv = 0.0;
-#pragma unroll
-                    for (int j = 0; j < 6; ++j) {
-                        sp = __dadd_rn(sp, __dmul_rn(kB[j], KP(j)[k * E + i]));
-                        sv = __dadd_rn(sv, __dmul_rn(kB[j], KV(j)[k * E + i]));
-                    }
-                    const double pn = __dadd_rn(Y0[k * Emax + i], __dmul_rn(hr, sp));
-                    const double vn = __dadd_rn(Y0[(3 + k) * Emax + i], __dmul_rn(hr, sv));
-                    NW[k * Emax + i] = pn;
-                    NW[(3 + k) * Emax + i] = vn;
-                    c.sp[k * E + i] = pn;
-                    KP(6)[k * E + i] = c.live[i] ? vn : 0.0;
-                }
-            }
-            __syncthreads();
-            c.key = (uint32_t)g * 2654435761u ^ (uint32_t)(gs.n_acc + gs.n_rej) * 40503u ^ 6u * 97u;
-            stage_accel<KIND, FORM, FAR>(c, KV(6), &s_flag);
             // embedded error norm (batched_rk45.py:372-393)
             double part = 0.0;
             for (int i = tid; i < E; i += nt) {

@@ -99,11 +99,18 @@ __device__ __forceinline__ void ring_field(double rho, double z, double a, doubl
 // several evaluations can be interleaved by the compiler.  For p >= 1e-3 the
 // sixth half-difference c_6 is below 1e-14, so a_6 has converged to the AGM
 // (its error is c_7 ~ 1e-28) and the neglected E-sum terms are below 1e-26.
+// The series branch (p < 1e-3: the point within ~3 % of the ring's radius
+// of the ring) out of line: it is rare in a far sum, and every interleaved
+// copy of the AGM below would otherwise carry its own copy of it.
+static __device__ __noinline__ void ellip_ke_series(double p, double& K, double& E) {
+    const double L = -0.5 * log(p);
+    K = fma(L, horner10(kSerK, p), horner10(kSerKd, p));
+    E = fma(0.5 * p, fma(L, horner10(kSerE, p), horner10(kSerEd, p)), 1.0);
+}
+
 __device__ __forceinline__ void ellip_ke_fixed(double p, double& K, double& E) {
     if (p < 1e-3) {
-        const double L = -0.5 * log(p);
-        K = fma(L, horner10(kSerK, p), horner10(kSerKd, p));
-        E = fma(0.5 * p, fma(L, horner10(kSerE, p), horner10(kSerEd, p)), 1.0);
+        ellip_ke_series(p, K, E);
         return;
     }
     double a = 1.0, b = sqrt(p);
@@ -121,6 +128,17 @@ __device__ __forceinline__ void ellip_ke_fixed(double p, double& K, double& E) {
     E = K * (1.0 - S);
 }
 
+// Near-axis Taylor branch of the ring field (rho^2 < 1e-10 (a^2 + z^2)), out
+// of line for the same reason as ellip_ke_series.
+static __device__ __noinline__ void ring_axis_taylor(double rho, double z, double a, double& er, double& ez) {
+    const double z2 = z * z, a2 = a * a, rho2 = rho * rho;
+    const double ax2 = a2 + z2;
+    const double s = sqrt(ax2);
+    const double ax15 = ax2 * s, ax25 = ax2 * ax15, ax35 = ax2 * ax25;
+    er = rho * (2.0 * z2 - a2) / (8.0 * kPi * ax25);
+    ez = z / (4.0 * kPi * ax15) + 3.0 * rho2 * z * (3.0 * a2 - 2.0 * z2) / (16.0 * kPi * ax35);
+}
+
 // Ring field for the far-quadrature sum: the formula of ring_field with one
 // reciprocal of D*d2 in place of the divisions by D and d2, and 1/rho
 // supplied by the caller (constant over a point's whole node loop).
@@ -130,11 +148,7 @@ __device__ __forceinline__ void ring_field_far(double rho, double inv_rho, doubl
     const double D = (rho + a) * (rho + a) + z2;
     const double d2 = (rho - a) * (rho - a) + z2;
     if (rho2 < 1e-10 * (a2 + z2)) {
-        const double ax2 = a2 + z2;
-        const double s = sqrt(ax2);
-        const double ax15 = ax2 * s, ax25 = ax2 * ax15, ax35 = ax2 * ax25;
-        er = rho * (2.0 * z2 - a2) / (8.0 * kPi * ax25);
-        ez = z / (4.0 * kPi * ax15) + 3.0 * rho2 * z * (3.0 * a2 - 2.0 * z2) / (16.0 * kPi * ax35);
+        ring_axis_taylor(rho, z, a, er, ez);
         return;
     }
     const double inv = 1.0 / (D * d2);
@@ -144,6 +158,12 @@ __device__ __forceinline__ void ring_field_far(double rho, double inv_rho, doubl
     const double rsD = sqrt(invD);
     er = (K - (a2 - rho2 + z2) * E * inv_d2) * (rsD * inv_rho * (1.0 / (4.0 * kPi * kPi)));
     ez = z * E * rsD * inv_d2 * (1.0 / (2.0 * kPi * kPi));
+}
+
+// ring_field_far out of line, for the rare float64 terms of a float32 sum.
+static __device__ __noinline__ void ring_field_far_cold(double rho, double inv_rho, double z, double a, double& er,
+                                                        double& ez) {
+    ring_field_far(rho, inv_rho, z, a, er, ez);
 }
 
 // ---------------------------------------------------------------------------

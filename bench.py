@@ -45,6 +45,8 @@ In the same run (rank 0):
               the final state, every step.
   cpu_baseline  the oracle port (the reference's algorithm) on the host
               cores, on a bounded prefix of the same trace.
+  image_force the BEM image-charge force per call (spt_image_force) at the
+              batch shapes the reference published timings for.
 
 N > 1 (torchrun): the workload is N x the groups (one draw of N x 4096
 groups for C1), split into contiguous group ranges balanced by estimated
@@ -478,14 +480,84 @@ def run_gpu(args, rank, world):
         e2e = e2e_leg(args, wl, tracer, pos, vel, tb, q, m, sizes, dev, t_max, budget)
     if rank == 0 and not args.no_plain and (args.form, args.far_rule) != ("fp64", "reference"):
         plain, acc = plain_and_accuracy(args, wl, pos, vel, tb, q, m, sizes, dev, t_max, budget)
+    img = image_force_leg(dev) if rank == 0 and not args.no_image else None
     peak = (fp64_peak_tflops if args.form == "fp64" else fp32_peak_tflops)(torch, dev) if rank == 0 else None
     flops = (dc["ring_far"] * FLOP_PER_RING + dc["ring_near"] * FLOP_PER_RING + dc["pair_evals"] * FLOP_PER_PAIR
              + dc["cluster_evals"] * FLOP_PER_CLUSTER)
     achieved = flops / t_total / 1e12
     return dict(value=steps_all / t_max_ranks, live=live_all / t_max_ranks, t_total=t_max_ranks, times=times,
                 counters=dc, clocks=clk.summary(), e2e=e2e, peak=peak, achieved=achieved, config=wl["config"],
-                plain=plain, accuracy=acc, tuned=tuned, t_max=t_max, ranges=ranges,
+                plain=plain, accuracy=acc, tuned=tuned, t_max=t_max, ranges=ranges, image_force=img,
                 launches_per_step=len(run.plan) if run.plan else 1)
+
+
+# The reference's own per-call image-force timings (docs/gpu_performance.md:21-29; RTX 5070 Ti, CuPy),
+# samples 1 nm outside the tip or above the well bottom: (geometry, G, E) -> ms per call
+IMAGE_PUBLISHED_MS = {("tip", 1, 1): 4.51, ("tip", 32, 4): 5.15, ("tip", 256, 4): 21.18,
+                      ("well", 1, 1): 4.28, ("well", 32, 4): 6.35, ("well", 256, 4): 19.81}
+
+
+def image_force_leg(dev, reps=7):
+    """spt_image_force per call (geometry level, the tables of
+    HemisphericalTipBEMGeometry(R = 50 nm, z0 = 3 nm) and
+    CylindricalWellBEMGeometry(R = 2 um, H = 1 um, z0 = 3 nm) with the
+    reference's default image parameters) at the batch shapes the reference
+    published, points 1 nm outside the tip / above the well floor: median of
+    `reps` CUDA-event-timed calls after a warm-up, inputs resident."""
+    import torch
+    from bem_b200 import _lib
+    from bem_b200 import image_charge as ic
+    from bem_b200.constants import COULOMB_CONSTANT, ELEMENTARY_CHARGE
+    rng = np.random.default_rng(7)
+    out = []
+    for geo_name in ("tip", "well"):
+        z0 = 3e-9
+        g = _lib.SptGeometry()
+        g.has_image, g.z0 = 1, z0
+        if geo_name == "tip":
+            R = 50e-9
+            prof = ic.tip_image_profile(R, z0, 5 * R, (R - z0) * np.pi / 2 / 29)
+            g.kind, g.R, g.z_handoff = _lib.GEOM_TIP_BEM, R, 20 * R
+        else:
+            R, H = 2e-6, 1e-6
+            room = min(0.5 * z0, 0.2 * (H - z0))
+            prof = ic.well_image_profile(R, H, z0, 5 * R, min(R, H) / 14, room, z0 + room)
+            g.kind, g.R, g.H, g.z_handoff = _lib.GEOM_WELL_BEM, R, H, 20 * R
+        sol = ic.ImageChargeSolution(prof, 16, 0.1 * R, 0.5 * R, device=dev)
+        for G, E in ((1, 1), (32, 4), (256, 4)):
+            n = G * E
+            if geo_name == "tip":
+                th = rng.uniform(0, np.radians(60), n)
+                ph = rng.uniform(-np.pi, np.pi, n)
+                r = R + 1e-9
+                pts = np.stack([r * np.sin(th) * np.cos(ph), r * np.sin(th) * np.sin(ph), r * np.cos(th)], -1)
+            else:
+                rr = 0.8 * R * np.sqrt(rng.uniform(0, 1, n))
+                ph = rng.uniform(-np.pi, np.pi, n)
+                pts = np.stack([rr * np.cos(ph), rr * np.sin(ph), np.full(n, -H + 1e-9)], -1)
+            pos = torch.as_tensor(pts, device=dev)
+            q = torch.full((n,), -ELEMENTARY_CHARGE, dtype=torch.float64, device=dev)
+            act = torch.ones(n, dtype=torch.uint8, device=dev)
+            off = torch.arange(0, n + 1, E, dtype=torch.int64, device=dev)
+            f = torch.empty((3, n), dtype=torch.float64, device=dev)
+            call = lambda: sol.force(pos, q, act, off, E, geometry=g, coulomb_constant=COULOMB_CONSTANT, out=f)
+            call()
+            torch.cuda.synchronize()
+            ts = []
+            st = torch.cuda.current_stream(dev)
+            for _ in range(reps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(st)
+                call()
+                b.record(st)
+                b.synchronize()
+                ts.append(a.elapsed_time(b))
+            ms = float(np.median(ts))
+            pub = IMAGE_PUBLISHED_MS[(geo_name, G, E)]
+            out.append(dict(geometry=geo_name, groups=G, group_size=E, ms_per_call=ms,
+                            reference_published_ms=pub, ratio=pub / ms))
+    return dict(what="geometry-level BEM image-charge force per call (spt_image_force, n_max 16); reference: "
+                     "its own published per-call times (RTX 5070 Ti, CuPy), not the same hardware", calls=out)
 
 
 def plain_and_accuracy(args, wl, pos, vel, tb, q, m, sizes, dev, t_max, budget):
@@ -646,6 +718,7 @@ def main():
                     help="mixed form: conditioning bound above which float32 sums are redone in float64 (0: 16)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-image", action="store_true", help="skip the per-call BEM image-charge force leg")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -698,6 +771,7 @@ def main():
         accuracy=r["accuracy"],
         counters=r["counters"],
         e2e=r["e2e"],
+        image_force=r["image_force"],
         cpu_baseline=cpu,
     )
     print(json.dumps(line))

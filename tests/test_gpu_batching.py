@@ -104,7 +104,7 @@ def test_autotune_picks_a_guarded_config_and_keeps_results():
         b = engine.GroupBatch(*arrays)
         res = None
         if tuned:
-            res = autotune.tune(tr, *arrays, *args, warm=8, attempts=4)
+            res = autotune.tune(tr, *arrays, *args, warm=8, attempts=4, tune_ratios=True)
             autotune.apply(res, tr, b)
         tr.launch(b, tr.params(*args, 30))
         torch.cuda.synchronize()
