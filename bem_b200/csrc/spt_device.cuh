@@ -1055,11 +1055,12 @@ __device__ __forceinline__ void near_point(Ctx& c, int k, unsigned long long& n_
 // form, float64 again when its sum is ill-conditioned.  The float64 tile is
 // the float64 form's, so with every sum redone the mixed form reproduces it.
 // Ring evaluations each lane keeps in flight in the float64 adaptive far sum.
-// Four, not eight: every in-flight evaluation is an inlined copy of the ring
-// kernel, and the trace kernel is bound by instruction fetch (measured: the
-// whole C1 trace 1.38x faster at four).
+// One: every in-flight evaluation is an inlined copy of the ring kernel, and
+// the trace kernel is bound by instruction fetch, not by the latency the
+// copies would hide (whole C1 traces, 1184 groups: 8 in flight 8.9 M, 4 in
+// flight 12.1 M, 2 in flight 15.4 M, 1 in flight 18.3 M particle-steps/s).
 #ifndef SPT_FAR_NQ_FP64
-#define SPT_FAR_NQ_FP64 4
+#define SPT_FAR_NQ_FP64 1
 #endif
 
 template <int FORM>

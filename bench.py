@@ -39,7 +39,10 @@ In the same run (rank 0):
               traces the same groups; ratio = chosen / plain on that subset.
   accuracy    endpoint error of the chosen form against the plain form on
               that subset (alive particles by position and velocity, killed
-              ones by death time), and their attempt counts.
+              ones by death time), and their attempt counts; beside it the
+              plain form's own sensitivity (the same subset with vel0 x
+              (1 + 1e-15)), and the error over the particles that sensitivity
+              shows to be well conditioned (moved < 1e-7 by it).
   e2e         the same whole traces through the public API with the state in
               pinned host memory: H2D of the initial state, the trace, D2H of
               the final state, every step.
@@ -576,6 +579,8 @@ def plain_and_accuracy(args, wl, pos, vel, tb, q, m, sizes, dev, t_max, budget):
     legs = [("plain", "fp64", "reference"), ("chosen", args.form, args.far_rule)]
     if args.form == "fp64" and args.far_rule == "adaptive":
         legs.append(("mixed", "mixed", "adaptive"))  # the float32 form, reported beside the chosen one
+    if not args.no_sensitivity:
+        legs.append(("plain_pert", "fp64", "reference"))  # the plain form's own sensitivity (vel0 x (1 + 1e-15))
     for name, form, rule in legs:
         tracer = make_tracer(args, wl, dev, form, rule)
         binned = False
@@ -586,7 +591,8 @@ def plain_and_accuracy(args, wl, pos, vel, tb, q, m, sizes, dev, t_max, budget):
                 autotune.apply(args.tuned_config, tracer)
             elif args.cta_threads:
                 tracer.cta_threads = args.cta_threads
-        run = Runner(tracer, *sub, dev, binned=binned)
+        leg = sub if name != "plain_pert" else (sub[0], sub[1] * (1.0 + 1e-15)) + sub[2:]
+        run = Runner(tracer, *leg, dev, binned=binned)
         prm = lambda a: tracer.params(t_max, wl["rtol"], wl["atol"], 1e-12, wl["cm"], a)
         # warm-up: a short slice, then the timed span from the initial state
         run.launch(prm(4), stream)
@@ -628,6 +634,21 @@ def plain_and_accuracy(args, wl, pos, vel, tb, q, m, sizes, dev, t_max, budget):
                max_rel_t_death=float(et.max()) if et.size else None,
                attempts_plain=int(P["c"]["attempts"]), attempts_chosen=int(C["c"]["attempts"]),
                accepted_steps_ratio=float(C["c"]["accepted"] / max(P["c"]["accepted"], 1)))
+    if "plain_pert" in out:
+        # endpoints are only as well defined as the trajectory allows: a 1e-15 change of vel0 moves the
+        # plain form's own endpoints by `sens`; the chosen form is held to 1e-6 where sens < 1e-7
+        d0, d1, d2 = P["td"], C["td"], out["plain_pert"]["td"]
+        alive_all = ~np.isfinite(d0) & ~np.isfinite(d1) & ~np.isfinite(d2)
+        rel = lambda X: np.linalg.norm(X["pos"] - P["pos"], axis=-1)[alive_all] / \
+            np.linalg.norm(P["pos"], axis=-1)[alive_all]
+        sens, err = rel(out["plain_pert"]), rel(C)
+        well = sens < 1e-7
+        acc["plain_self_sensitivity"] = dict(
+            what="plain form against itself with vel0 x (1 + 1e-15), alive particles", max_rel_pos=float(sens.max()),
+            particles_above_1e6=int((sens > 1e-6).sum()), seconds=out["plain_pert"]["t"])
+        acc["max_rel_pos_well_conditioned"] = float(err[well].max()) if well.any() else None
+        acc["well_conditioned_particles"] = int(well.sum())
+        acc["max_error_over_sensitivity"] = float((err / np.maximum(sens, 1e-7)).max())
     if "mixed" in out:
         X = out["mixed"]
         e = errors(X)
@@ -719,6 +740,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-image", action="store_true", help="skip the per-call BEM image-charge force leg")
+    ap.add_argument("--no-sensitivity", action="store_true",
+                    help="skip the perturbed plain run that measures the trajectories' own conditioning")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
