@@ -17,6 +17,7 @@ FORM_FP64, FORM_MIXED, FORM_SURROGATE = 0, 1, 2
 FAR_REFERENCE, FAR_ADAPTIVE = 0, 1
 FAR_RULES = {"reference": FAR_REFERENCE, "adaptive": FAR_ADAPTIVE}
 GROUP_NEW, GROUP_RUNNING, GROUP_DONE, GROUP_NONFINITE, GROUP_TIMEOUT = 0, 1, 2, 3, 4
+TEAM_AUTO, TEAM_CTA, TEAM_WARP = 0, 1, 2
 COUNTERS = ("attempts", "accepted", "particle_steps", "stage_evals", "pair_evals", "ring_far", "ring_near",
             "near_pairs", "fp64_rounds", "fp64_targets", "live_steps", "cluster_evals")
 N_COUNTERS = len(COUNTERS)
@@ -69,7 +70,7 @@ class SptTraceParams(ctypes.Structure):
                 ("output_flag", _p), ("sur_w", _p), ("sur_w16", _p), ("sur_s_start", _p), ("sur_log_scale", _p),
                 ("sur_s_end", _d), ("sur_sig_floor", _d), ("sur_band", _d), ("sur_spot", _d), ("sur_d_min", _d),
                 ("sur_d_max", _d), ("sur_stats", _p), ("round_points", _i32), ("cta_threads", _i32), ("kappa_max", _d),
-                ("max_ctas", _i32), ("reserved3", _i32)]
+                ("max_ctas", _i32), ("team", _i32)]
 
 
 class SptAccelArgs(ctypes.Structure):
@@ -88,7 +89,7 @@ class SptGemmArgs(ctypes.Structure):
 
 IMAGE_MAX_MODES = 64
 TRACE_IMAGE_MODES = 16
-ABI_VERSION = 3
+ABI_VERSION = 4
 EPI_STORE, EPI_BIAS_SILU, EPI_DSILU = 0, 1, 2
 _f = ctypes.c_float
 

@@ -6,6 +6,11 @@ The knobs change speed, not physics:
   time): narrower CTAs put more groups on an SM and fewer warps behind each
   barrier; wider ones spread a large group's work.  Results agree to the
   summation order of the reductions.
+* ``team`` -- one group per warp (lane i = particle i, several groups per
+  CTA, no CTA barrier inside a group's step) or one group per CTA, where
+  the warp team is offered (BEM geometry without the image-charge force,
+  float64, adaptive far rule, groups of at most 32).  Results agree to the
+  summation order of the pair sums.
 * ``round_points`` -- the far-sum tile shape: evaluation points per round
   (1, 2, 4).  Fewer points give each thread more nodes in flight per
   point; more points share node loads and the adaptive rule's
@@ -29,7 +34,7 @@ Procedure: a sample of groups (every k-th group, so that every size range is
 represented; 2368 = 16 per SM, enough to fill the GPU at every CTA width) is
 advanced `warm` attempts from emission, the warmed state is saved, and each
 candidate runs `attempts` attempts from that state, timed with CUDA events
-(best of `repeats`).  Coordinate descent: cta_threads, round_points, then
+(best of `repeats`).  Coordinate descent: team, cta_threads, round_points, then
 ratios; a candidate replaces the current choice only if it is faster by more
 than `margin` (timing noise on a sample is a few per cent).  The winner
 is applied to a Tracer / GroupBatch with ``apply``.  Results can be cached
@@ -65,7 +70,19 @@ def signature(tracer, sizes):
 
 
 class TuneResult(dict):
-    """config (cta_threads, round_points, ratios, order) plus the timings behind it."""
+    """config (team, cta_threads, round_points, ratios, order) plus the timings behind it."""
+
+
+def warp_team_offered(tracer, sizes):
+    """Whether the library offers the warp team for this tracer and group
+    sizes (the predicate of the C ABI's team selection)."""
+    if tracer.tables is None or tracer.bem is None or tracer.far_rule != "adaptive" or tracer.form != _lib.FORM_FP64:
+        return False
+    if int(np.max(sizes)) > 32:
+        return False
+    bem_image = (tracer.geom.kind in (_lib.GEOM_TIP_BEM, _lib.GEOM_WELL_BEM) and tracer.geom.has_image
+                 and tracer.bem.image.n_nodes >= 2)
+    return not bem_image
 
 
 def _sample(sizes, n_sample):
@@ -112,14 +129,15 @@ def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plum
     sub = (np.asarray(pos)[rows], np.asarray(vel)[rows], np.asarray(t_birth)[rows], np.asarray(charge)[rows],
            np.asarray(mass)[rows], sizes[groups])
     base = engine.GroupBatch(*sub, device=tracer.device)
-    prm = lambda a, rp=None, th=None: tracer.params(t_max, rtol, atol, plummer_radius, charge_to_mass, a,
-                                                    round_points=rp, cta_threads=th)
+    prm = lambda a, rp=None, th=None, tm=None: tracer.params(t_max, rtol, atol, plummer_radius, charge_to_mass, a,
+                                                             round_points=rp, cta_threads=th, team=tm)
     tracer.launch(base, prm(warm))
     torch.cuda.synchronize()
     work = engine.GroupBatch(*sub, device=tracer.device)
-    saved_bem, saved_rp, saved_th = tracer.bem, tracer.round_points, tracer.cta_threads
+    saved_bem, saved_rp, saved_th, saved_tm = tracer.bem, tracer.round_points, tracer.cta_threads, tracer.team
 
-    def timed(order, rp, ratios, th=0):
+    def timed(order, rp, ratios, th=0, tm=None):
+        tm = cfg["team"] if tm is None else tm
         if tracer.tables is not None:
             tracer.bem = tracer.tables.view(tracer.far_rule, ratio4=ratios[0], ratio2=ratios[1], ratio_run=ratios[2])
         work.set_order(order)
@@ -130,7 +148,7 @@ def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plum
             c0 = tracer.counter_dict()["particle_steps"]
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record()
-            tracer.launch(work, prm(attempts, rp, th))
+            tracer.launch(work, prm(attempts, rp, th, tm))
             e.record()
             e.synchronize()
             best = min(best, s.elapsed_time(e) * 1e-3)
@@ -138,13 +156,18 @@ def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plum
         return steps / best
 
     timings = {}
-    cfg = dict(cta_threads=0, round_points=4, ratios=list(RATIOS[0]), order="largest_first")
+    cfg = dict(team=_lib.TEAM_AUTO, cta_threads=0, round_points=4, ratios=list(RATIOS[0]), order="largest_first")
 
     def pick(rates, current):
         best = max(rates, key=rates.get)
         return best if rates[best] > (1.0 + margin) * rates[current] else current
 
     try:
+        if warp_team_offered(tracer, sizes):
+            rates = {}
+            for tm, name in ((_lib.TEAM_WARP, "warp"), (_lib.TEAM_CTA, "cta")):
+                rates[tm] = timings[f"team={name}"] = timed(cfg["order"], cfg["round_points"], cfg["ratios"], 0, tm)
+            cfg["team"] = max(rates, key=rates.get)
         if len(threads) > 1 or threads[0]:
             rates = {}
             for th in threads:
@@ -167,7 +190,7 @@ def tune(tracer, pos, vel, t_birth, charge, mass, sizes, t_max, rtol, atol, plum
             elif rates:
                 cfg["ratios"] = list(max(rates, key=rates.get))
     finally:
-        tracer.bem, tracer.round_points, tracer.cta_threads = saved_bem, saved_rp, saved_th
+        tracer.bem, tracer.round_points, tracer.cta_threads, tracer.team = saved_bem, saved_rp, saved_th, saved_tm
     res = TuneResult(cfg, timings=timings, key=key, sample_groups=len(groups), attempts=attempts, warm=warm)
     if cache:
         stored = {}
@@ -184,6 +207,7 @@ def apply(config, tracer, batch=None):
     """Set a tuned configuration on a Tracer (and a GroupBatch's order)."""
     tracer.round_points = int(config["round_points"])
     tracer.cta_threads = int(config.get("cta_threads", 0))
+    tracer.team = int(config.get("team", _lib.TEAM_AUTO))
     if tracer.tables is not None:
         r = config["ratios"]
         tracer.bem = tracer.tables.view(tracer.far_rule, ratio4=r[0], ratio2=r[1], ratio_run=r[2])

@@ -638,8 +638,8 @@ __device__ __forceinline__ void cluster_field(const double* rec, int nt, double 
     double p0 = 1.0, p1 = u, d0 = 0.0, d1 = 1.0;
     double A = __ldg(rec + 2), B = 0.0;
     double xn = x;
-    for (int n = 1; n < nt; ++n) {
-        const double m = __ldg(rec + 2 + n) * xn;
+    auto term = [&](int n, double moment) {
+        const double m = moment * xn;
         A = fma((double)(n + 1) * m, p1, A);
         B = fma(m, d1, B);
         const double p2 = fma(kLegA[n] * u, p1, -kLegB[n] * p0);
@@ -649,7 +649,18 @@ __device__ __forceinline__ void cluster_field(const double* rec, int nt, double 
         d0 = d1;
         d1 = d2;
         xn *= x;
+    };
+    // moments loaded four terms ahead of the recurrence that consumes them
+    int n = 1;
+    for (; n + 3 < nt; n += 4) {
+        const double m0 = __ldg(rec + 2 + n), m1 = __ldg(rec + 3 + n), m2 = __ldg(rec + 4 + n),
+                     m3 = __ldg(rec + 5 + n);
+        term(n, m0);
+        term(n + 1, m1);
+        term(n + 2, m2);
+        term(n + 3, m3);
     }
+    for (; n < nt; ++n) term(n, __ldg(rec + 2 + n));
     const double sc = ir * ir * 0.07957747154594767;  // 1 / (4 pi r^2)
     const double e_r = A * sc, e_t = s * B * sc;
     er = e_r * s + e_t * u;
@@ -920,17 +931,32 @@ __device__ __forceinline__ void closest_point(Ctx& c, int k, bool frame) {
             // minimum; only runs whose lower bound does not exceed it are scanned
             // (each lane still takes its segments in increasing order)
             const int nblk = (nseg + SPT_BLOCK_SEGS - 1) / SPT_BLOCK_SEGS;
-            double lbm = INFINITY;
+            double lbm = INFINITY, lmx = 0.0;
             int qm = 0;
             for (int q = lane; q < nblk; q += 32) {
                 const double lb = blk_lower(b, q, rho, z);
                 if (lb < lbm) { lbm = lb; qm = q; }
+                lmx = fmax(lmx, blk_lmax(b, q));
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 const double ol = __shfl_xor_sync(0xffffffffu, lbm, o);
                 const int oq = __shfl_xor_sync(0xffffffffu, qm, o);
                 if (ol < lbm || (ol == lbm && oq < qm)) { lbm = ol; qm = oq; }
+                lmx = fmax(lmx, __shfl_xor_sync(0xffffffffu, lmx, o));
+            }
+            // Every segment at least 2e-9 x the longest segment away (the run
+            // bounds are rigorous lower bounds): the on-surface offset below
+            // (distance^2 < (1e-9 L)^2) cannot apply, the closest segment
+            // plays no further part, and the evaluation point is the point
+            // itself -- the offset path's rho + 0 and z + 0 bit for bit (z = 0
+            // excepted: there the sign of the zero would follow the normal).
+            if (!frame && z != 0.0 && lbm > 2e-9 * lmx) {
+                if (lane == 0) {
+                    P[8 * k + 3] = rho;
+                    P[8 * k + 4] = z;
+                }
+                return;
             }
             double ub = INFINITY;
             if (qm * SPT_BLOCK_SEGS + lane < nseg) ub = seg_dist2(b, qm * SPT_BLOCK_SEGS + lane, rho, z);
@@ -2253,6 +2279,489 @@ accel_kernel(const __grid_constant__ SptAccelArgs a, const __grid_constant__ Spt
 }
 
 // ---------------------------------------------------------------------------
+// One group per warp, several groups per CTA, the CTA's BEM points pooled
+// (groups of at most 32 particles, BEM geometries without the BEM
+// image-charge force, float64 form, adaptive far rule).
+//
+// Lane i of a warp is particle i of the warp's group: stage combination,
+// pair sums (one target per lane, sources in order), error norm, controller,
+// kills, screens and output times run per warp, with the group scalars held
+// alike by every lane (sums over the group taken in lane 0 and broadcast).
+// The CTA's warps advance their groups through each stage in step, and the
+// BEM points of all of them go into one CTA-wide task pool that every warp
+// draws from (closest segment, near quadrature, adaptive far sum -- the CTA
+// team's warp routines, so the same field to the bit -- and the rotation,
+// written back to the owning group).  With one group per CTA, warps that had
+// finished their share of a stage's points idled at the barrier behind the
+// slowest point; with one free-running group per warp, the warps' scattered
+// positions in the stage code thrashed the instruction cache.  Here the pool
+// of ~W x 17 points balances to within one point, warps share their
+// instruction stream, and warps whose group is done help with the others'
+// points until the work queue is empty.  The step's state -- y0, the
+// 5th-order solution and the seven stage slopes -- lives in a per-warp slot
+// in global memory (component k of lane i at slot[k * 32 + i], coalesced),
+// read and written past L1 so that L1 keeps the BEM tables.
+
+constexpr int kWarpSlotComps = 54;  // y0 6, 5th-order solution 6, stage velocities 21, stage accelerations 21
+constexpr int kWarpSlotDoubles = kWarpSlotComps * 32;
+// per-warp shared doubles: BEM record 8, near-sum scratch 4, stage positions
+// and charges 4 x 32, sphere images 4 x 32, BEM fields 3 x 32, live flags 32 ints
+constexpr int kWarpTeamDoubles = 8 + 4 + 4 * 32 + 4 * 32 + 3 * 32 + 16;
+
+__host__ __device__ inline size_t warp_team_smem(int warps) {
+    return (size_t)warps * ((size_t)kWarpScratchInts * 4 + (size_t)kWarpTeamDoubles * 8);
+}
+
+__device__ __forceinline__ double warp_min_all(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;  // min is exact and order-free: every lane holds the same value
+}
+
+// per-warp shared region of warp w
+struct WarpTeam {
+    double *rec, *nfld, *sx, *sy, *sz, *q, *img, *fld;
+    int* live;
+    __device__ WarpTeam(double* smem, int nw, int w) {
+        double* t = smem + (size_t)nw * kWarpScratchInts / 2 + (size_t)w * kWarpTeamDoubles;
+        rec = t;
+        nfld = t + 8;
+        sx = t + 12;
+        sy = sx + 32;
+        sz = sy + 32;
+        q = sz + 32;
+        img = q + 32;
+        fld = img + 128;
+        live = reinterpret_cast<int*>(fld + 96);
+    }
+};
+
+// The CTA's BEM task pool of one stage: entries (warp << 5 | particle),
+// drawn one per warp task; every warp calls, between the barriers that close
+// the appends and open the next stage.
+template <int FORM>
+__device__ __forceinline__ void pool_bem_points(Ctx& c, double* smem, const int* entries, int count, int* next) {
+    const int lane = threadIdx.x & 31;
+    double* const P = c.bpt;
+    unsigned long long n_near = 0, n_ring_near = 0, far_evals = 0, cl_evals = 0;
+    for (;;) {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(next, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= count) break;
+        const int e = entries[t];
+        const WarpTeam own(smem, c.nw, e >> 5);
+        const int k = e & 31;
+        if (lane == 0) {
+            P[0] = own.sx[k];
+            P[1] = own.sy[k];
+            P[2] = own.sz[k];
+        }
+        __syncwarp();
+        closest_point(c, 0, false);
+        __syncwarp();
+        near_point(c, 0, n_near, n_ring_near);
+        __syncwarp();
+        far_point<FORM>(c, 0, far_evals, cl_evals);
+        __syncwarp();
+        if (lane == 0) {  // rotation to (x, y), as bem_points_fused
+            const double x = P[0], y = P[1];
+            const double rho = hypot(x, y);
+            const double e_rho = P[5];
+            double ex = 0.0, ey = 0.0;
+            if (rho != 0.0) {
+                ex = e_rho * (x / rho);
+                ey = e_rho * (y / rho);
+            }
+            own.fld[3 * k + 0] = ex;
+            own.fld[3 * k + 1] = ey;
+            own.fld[3 * k + 2] = P[6];
+        }
+        __syncwarp();
+    }
+    count_add(c, SPT_CNT_NEAR_PAIRS, n_near);
+    count_add(c, SPT_CNT_RING_NEAR, n_ring_near);
+    count_add(c, SPT_CNT_RING_FAR, far_evals);
+    count_add(c, SPT_CNT_CLUSTER_EVALS, cl_evals);
+}
+
+// The rest of a stage for this warp's group, after the pool: images, pair
+// sums and the blended external field into this lane's acceleration.
+template <int KIND>
+__device__ __forceinline__ void stage_finish_warp(Ctx& c, const WarpTeam& w, bool live, bool need, double xi,
+                                                  double yi, double zi, double mi, double& ax, double& ay,
+                                                  double& az) {
+    const int lane = threadIdx.x & 31, E = c.E;
+    const SptGeometry& g = c.g;
+    // image sources of the sphere-on-plane construction (forces.py:170-183)
+    const bool three_img = KIND == SPT_GEOM_POST_BEM && g.has_image;
+    const double zc = (KIND == SPT_GEOM_POST_BEM) ? g.L : 0.0;
+    if (three_img) {
+        if (lane < E) {
+            const double a = g.R - g.z0;
+            const double x = xi, y = yi, z = zi - zc;
+            const double d = sqrt(x * x + y * y + z * z);
+            const double ds = d > 0.0 ? d : a;
+            const double sh = (a * a) / (ds * ds);
+            w.img[lane] = x * sh;
+            w.img[32 + lane] = y * sh;
+            w.img[64 + lane] = z * sh;
+            w.img[96 + lane] = -w.q[lane] * (a / ds);
+        }
+        __syncwarp();
+    }
+    // pair sums, one target per lane, sources in order (forces.py:16-57,
+    // 101-191), and the blended external field
+    ax = ay = az = 0.0;
+    unsigned long long pairs = 0;
+    if (live) {
+        const double qk = c.kc * w.q[lane];
+        double fcx = 0.0, fcy = 0.0, fcz = 0.0, fix = 0.0, fiy = 0.0, fiz = 0.0;
+        if (E > 1) {
+            auto real = [&](int j, double& x, double& y, double& z, double& q) {
+                x = w.sx[j]; y = w.sy[j]; z = w.sz[j]; q = w.q[j];
+            };
+            pair_sum<false>(c, E, 0, 1, xi, yi, zi, qk, real, fcx, fcy, fcz);
+            pairs += E;
+        }
+        if (three_img) {
+            const double pz0 = g.L + g.z0;
+            const double zl = zi - zc;
+            double s1x, s1y, s1z, s2x, s2y, s2z, s3x, s3y, s3z;
+            auto sphere = [&](int j, double& x, double& y, double& z, double& q) {
+                x = w.img[j]; y = w.img[32 + j]; z = w.img[64 + j]; q = w.img[96 + j];
+            };
+            auto plane = [&](int j, double& x, double& y, double& z, double& q) {
+                x = w.sx[j]; y = w.sy[j]; z = -2.0 * pz0 - (w.sz[j] - zc); q = -w.q[j];
+            };
+            auto plane_sphere = [&](int j, double& x, double& y, double& z, double& q) {
+                x = w.img[j]; y = w.img[32 + j]; z = -2.0 * pz0 - w.img[64 + j]; q = -w.img[96 + j];
+            };
+            pair_sum<false>(c, E, 0, 1, xi, yi, zl, qk, sphere, s1x, s1y, s1z);
+            pair_sum<false>(c, E, 0, 1, xi, yi, zl, qk, plane, s2x, s2y, s2z);
+            pair_sum<false>(c, E, 0, 1, xi, yi, zl, qk, plane_sphere, s3x, s3y, s3z);
+            fix = (s1x + s2x) + s3x;
+            fiy = (s1y + s2y) + s3y;
+            fiz = (s1z + s2z) + s3z;
+            pairs += 3 * E;
+        }
+        // blend(near, far) with near = where(valid, uniform + pert, 0) (bem/geometry.py:44-55, bem/fields.py:186-211)
+        const double wgt = blend_weight(zi, g.z_handoff);
+        const bool valid = bem_valid<KIND>(xi, yi, zi, g);
+        const double fz = (zi >= 0.0) ? g.E_gun : 0.0;
+        double nx = 0.0, ny = 0.0, nz = 0.0;
+        if (valid && wgt > 0.0) {
+            const double bx = need ? w.fld[3 * lane + 0] : 0.0;
+            const double by = need ? w.fld[3 * lane + 1] : 0.0;
+            const double bz = need ? w.fld[3 * lane + 2] : 0.0;
+            nx = 0.0 + bx;
+            ny = 0.0 + by;
+            nz = g.E_gun + bz;
+        } else if (valid) {
+            nx = 0.0; ny = 0.0; nz = g.E_gun;
+        }
+        const double ex = wgt * nx + (1.0 - wgt) * 0.0;
+        const double ey = wgt * ny + (1.0 - wgt) * 0.0;
+        const double ez = wgt * nz + (1.0 - wgt) * fz;
+        ax = (c.cm * ex + fcx / mi) + fix / mi;
+        ay = (c.cm * ey + fcy / mi) + fiy / mi;
+        az = (c.cm * ez + fcz / mi) + fiz / mi;
+    }
+    count_add(c, SPT_CNT_PAIR_EVALS, pairs);
+}
+
+template <int KIND, int FORM>
+__global__ void __launch_bounds__(kMaxThreads, 2)
+trace_warp_kernel(const __grid_constant__ SptState st, const __grid_constant__ SptTraceParams prm,
+                  const __grid_constant__ SptGeometry geo, const __grid_constant__ SptBem bem, int* work,
+                  double* slots) {
+    static_assert(FORM == SPT_FORM_FP64, "the warp team runs the float64 form");
+    extern __shared__ __align__(16) double smem[];
+    __shared__ unsigned long long s_cnt[SPT_N_COUNTERS];
+    __shared__ int s_pool[2][kMaxThreads];  // two stages' task pools, used alternately
+    __shared__ int s_pool_n[2], s_pool_next[2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = threadIdx.x; k < SPT_N_COUNTERS; k += blockDim.x) s_cnt[k] = 0;
+    if (threadIdx.x < 2) s_pool_n[threadIdx.x] = s_pool_next[threadIdx.x] = 0;
+    Ctx c(geo, bem);
+    c.cm = prm.charge_to_mass;
+    c.kc = prm.coulomb_constant;
+    c.soft2 = prm.plummer_radius * prm.plummer_radius;
+    c.kappa = prm.kappa_max > 0.0 ? prm.kappa_max : kKappa;
+    c.round_pts = 1;
+    c.cnt = s_cnt;
+    c.nt = blockDim.x;
+    c.nw = nw;
+    c.tiles = smem;  // far-rule scratch of every warp (far_adaptive_warp takes its own by warp index)
+    const WarpTeam w(smem, nw, warp);
+    c.bpt = w.rec;
+    c.fld = w.nfld;
+    c.live = w.live;
+    double* const slot = slots + ((size_t)blockIdx.x * nw + warp) * kWarpSlotDoubles + lane;
+    auto ld = [&](int k) { return __ldcg(slot + 32 * k); };
+    auto sto = [&](int k, double v) { __stcg(slot + 32 * k, v); };
+    constexpr int Y0 = 0, NW = 6, KP = 12, KV = 33;
+    __syncthreads();
+
+    const int n_run = st.n_active ? *st.n_active : st.n_groups;
+    // this warp's group and its scalars (alike in every lane)
+    bool have = false, queue_empty = false;
+    int g = 0, E = 0, status = 0;
+    long long base = 0, pi = 0, n_acc = 0, n_rej = 0, att = 0;
+    bool in = false;
+    double tb = INFINITY, td = INFINITY, mi = 1.0, t = 0.0, h = 0.0;
+    auto write_back = [&]() {
+        if (in) {
+            st.x[pi] = ld(Y0 + 0); st.y[pi] = ld(Y0 + 1); st.z[pi] = ld(Y0 + 2);
+            st.vx[pi] = ld(Y0 + 3); st.vy[pi] = ld(Y0 + 4); st.vz[pi] = ld(Y0 + 5);
+            st.t_death[pi] = td;
+        }
+        if (lane == 0) {
+            st.t[g] = t;
+            st.h[g] = h;
+            st.status[g] = status;
+            st.n_accepted[g] = n_acc;
+            st.n_rejected[g] = n_rej;
+        }
+        have = false;
+    };
+    int tick = 0;  // stages taken by the CTA (the pool parity)
+    for (;;) {
+        // ready this warp's group for an attempt: take groups from the work
+        // queue until one is running and within this call's attempt budget
+        double hr = 0.0, next_cp = 0.0, next_out = 0.0;
+        bool exhausted = true, out_exh = true;
+        int out_ptr = 0;
+        for (;;) {
+            if (!have) {
+                if (queue_empty) break;
+                int gi = 0;
+                if (lane == 0) gi = atomicAdd(work, 1);
+                gi = __shfl_sync(0xffffffffu, gi, 0);
+                if (gi >= n_run) { queue_empty = true; break; }
+                g = st.group_order ? st.group_order[gi] : gi;
+                base = st.group_offset[g];
+                E = (int)(st.group_offset[g + 1] - base);
+                status = st.status[g];
+                if (E <= 0 || E > 32 || status >= SPT_GROUP_DONE) continue;
+                in = lane < E;
+                pi = base + (in ? lane : 0);
+                tb = in ? st.t_birth[pi] : INFINITY;
+                td = in ? st.t_death[pi] : INFINITY;
+                mi = in ? st.mass[pi] : 1.0;
+                __syncwarp();  // the previous group's last pair sums have read q
+                w.q[lane] = in ? st.charge[pi] : 0.0;
+                if (in) {
+                    sto(Y0 + 0, st.x[pi]); sto(Y0 + 1, st.y[pi]); sto(Y0 + 2, st.z[pi]);
+                    sto(Y0 + 3, st.vx[pi]); sto(Y0 + 4, st.vy[pi]); sto(Y0 + 5, st.vz[pi]);
+                }
+                t = st.t[g];
+                h = st.h[g];
+                n_acc = st.n_accepted[g];
+                n_rej = st.n_rejected[g];
+                att = 0;
+                have = true;
+                int fire_out = -1;
+                if (status == SPT_GROUP_NEW) {
+                    // start at the first birth (batched_rk45.py:164-178)
+                    t = warp_min_all(tb);
+                    h = (prm.t_max - t) * prm.initial_step_fraction;
+                    status = t < prm.t_max ? SPT_GROUP_RUNNING : SPT_GROUP_DONE;
+                    if (prm.n_outputs > 0) {
+                        const int last = count_le(prm.output_times, prm.n_outputs, t) - 1;
+                        if (last >= 0 && prm.output_times[last] == t) fire_out = last;
+                    }
+                }
+                if (fire_out >= 0 && in && tb <= t) {
+                    double sv[6];
+                    for (int k = 0; k < 6; ++k) sv[k] = ld(Y0 + k);
+                    write_output(prm, st.n_particles, fire_out, base + lane, t, sv);
+                }
+            }
+            if (status != SPT_GROUP_RUNNING || att >= prm.max_attempts) {
+                write_back();
+                continue;
+            }
+            // next checkpoint: the first birth after t (batched_rk45.py:228-242)
+            const double ncp = warp_min_all(tb > t ? tb : INFINITY);
+            exhausted = !(ncp < INFINITY);
+            next_cp = exhausted ? prm.t_max : ncp;
+            double target = fmin(next_cp, prm.t_max);
+            out_ptr = 0;
+            out_exh = true;
+            next_out = prm.t_max;
+            if (prm.n_outputs > 0) {
+                out_ptr = count_le(prm.output_times, prm.n_outputs, t);
+                out_exh = out_ptr >= prm.n_outputs;
+                next_out = out_exh ? prm.t_max : prm.output_times[out_ptr];
+                target = fmin(target, next_out);
+            }
+            hr = fmin(h, target - t);
+            if (!(hr > 0.0) || !isfinite(hr)) {
+                status = SPT_GROUP_NONFINITE;
+                write_back();
+                continue;
+            }
+            break;
+        }
+        const bool run = have;
+        if (!__syncthreads_or(run)) break;
+        c.E = E;
+        const bool live = run && in && (t >= tb) && (t < td);
+        // seven stage evaluations (batched_rk45.py:326-370), in step across the CTA
+        for (int s = 0; s < 7; ++s, ++tick) {
+            const int pp = tick & 1;
+            double px = 0.0, py = 0.0, pz = 0.0;
+            bool need = false;
+            if (run) {
+                if (in) {
+                    if (s < 6) {
+                        double p[6];
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) p[k] = ld(Y0 + k);
+                        for (int j = 0; j < s; ++j) {
+                            const double a = kA[s][j];
+                            if (a == 0.0) continue;
+                            const double ha = __dmul_rn(hr, a);
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                p[k] = __dadd_rn(p[k], __dmul_rn(ha, ld(KP + 3 * j + k)));
+                                p[3 + k] = __dadd_rn(p[3 + k], __dmul_rn(ha, ld(KV + 3 * j + k)));
+                            }
+                        }
+                        px = p[0]; py = p[1]; pz = p[2];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) sto(KP + 3 * s + k, live ? p[3 + k] : 0.0);
+                    } else {
+                        double pn[3];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            double sp = 0.0, sv = 0.0;
+#pragma unroll
+                            for (int j = 0; j < 6; ++j) {
+                                sp = __dadd_rn(sp, __dmul_rn(kB[j], ld(KP + 3 * j + k)));
+                                sv = __dadd_rn(sv, __dmul_rn(kB[j], ld(KV + 3 * j + k)));
+                            }
+                            pn[k] = __dadd_rn(ld(Y0 + k), __dmul_rn(hr, sp));
+                            const double vn = __dadd_rn(ld(Y0 + 3 + k), __dmul_rn(hr, sv));
+                            sto(NW + k, pn[k]);
+                            sto(NW + 3 + k, vn);
+                            sto(KP + 18 + k, live ? vn : 0.0);
+                        }
+                        px = pn[0]; py = pn[1]; pz = pn[2];
+                    }
+                }
+                w.sx[lane] = px;
+                w.sy[lane] = py;
+                w.sz[lane] = pz;
+                w.live[lane] = live;
+                // the BEM field of the live particles inside the valid region
+                // with blend weight > 0 goes to the CTA's pool
+                need = live && bem_valid<KIND>(px, py, pz, geo) && blend_weight(pz, geo.z_handoff) > 0.0;
+                const unsigned m = __ballot_sync(0xffffffffu, need);
+                int at = 0;
+                if (lane == 0 && m) at = atomicAdd(&s_pool_n[pp], __popc(m));
+                at = __shfl_sync(0xffffffffu, at, 0);
+                if (need) s_pool[pp][at + __popc(m & ((1u << lane) - 1u))] = (warp << 5) | lane;
+            }
+            __syncthreads();
+            // the other pool is free until the next stage's appends, which follow the barrier below
+            if (threadIdx.x == 0) {
+                s_pool_n[pp ^ 1] = 0;
+                s_pool_next[pp ^ 1] = 0;
+            }
+            pool_bem_points<FORM>(c, smem, s_pool[pp], s_pool_n[pp], &s_pool_next[pp]);
+            __syncthreads();
+            if (run) {
+                double ax, ay, az;
+                stage_finish_warp<KIND>(c, w, live, need, px, py, pz, mi, ax, ay, az);
+                if (in) {
+                    sto(KV + 3 * s + 0, ax);
+                    sto(KV + 3 * s + 1, ay);
+                    sto(KV + 3 * s + 2, az);
+                }
+                __syncwarp();  // the positions and images are rewritten by the next stage
+            }
+        }
+        if (!run) continue;
+        // embedded error norm (batched_rk45.py:372-393); the sum over the
+        // group in lane 0, as the CTA kernel's fixed-order block sum
+        double part = 0.0;
+        if (in) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                double ep = 0.0, ev = 0.0;
+#pragma unroll
+                for (int j = 0; j < 7; ++j) {
+                    ep = __dadd_rn(ep, __dmul_rn(kE[j], ld(KP + 3 * j + k)));
+                    ev = __dadd_rn(ev, __dmul_rn(kE[j], ld(KV + 3 * j + k)));
+                }
+                ep = __dmul_rn(hr, ep);
+                ev = __dmul_rn(hr, ev);
+                const double y0p = ld(Y0 + k), nwp = ld(NW + k);
+                const double y0v = ld(Y0 + 3 + k), nwv = ld(NW + 3 + k);
+                const double scp = __dadd_rn(prm.atol, __dmul_rn(prm.rtol, fmax(fabs(y0p), fabs(nwp))));
+                const double scv = __dadd_rn(kSpeedOfLight * prm.atol, __dmul_rn(prm.rtol, fmax(fabs(y0v), fabs(nwv))));
+                const double a = __ddiv_rn(ep, scp), b = __ddiv_rn(ev, scv);
+                part = __dadd_rn(part, __dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+            }
+        }
+        const double sq = 0.0 + __shfl_sync(0xffffffffu, warp_sum(part), 0);
+        double err = sqrt(sq / (double)(6 * E));
+        if (err == 0.0) err = kTiny;
+        const bool accepted = err <= 1.0;
+        double fac = prm.safety * pow(err, -1.0 / 5.0);
+        fac = fmin(fmax(fac, prm.min_factor), prm.max_factor);
+        const double h_next = hr * fac;
+        if (lane == 0) {
+            const long long k_att = n_acc + n_rej;
+            if (prm.log_capacity > 0 && k_att < prm.log_capacity) {
+                prm.log_h[(size_t)g * prm.log_capacity + k_att] = hr;
+                prm.log_err[(size_t)g * prm.log_capacity + k_att] = err;
+            }
+            atomicAdd(c.cnt + SPT_CNT_ATTEMPTS, 1ull);
+            atomicAdd(c.cnt + SPT_CNT_STAGE_EVALS, 7ull * E);
+        }
+        if (accepted) {
+            const double t_new = t + hr;
+            const double dt = t_new - t;
+            const double tol_out = 1e-9 * fmax(prm.t_max, 1e-30);
+            const bool hit = prm.n_outputs > 0 && !out_exh && t_new >= next_out - tol_out;
+            if (in) {
+                double o[6], nv[6];
+#pragma unroll
+                for (int k = 0; k < 6; ++k) { o[k] = ld(Y0 + k); nv[k] = ld(NW + k); }
+                if (live && kill_test<KIND>(nv[0], nv[1], nv[2], geo)) td = t_new;
+                if (hit && tb <= t_new) write_output(prm, st.n_particles, out_ptr, base + lane, t_new, nv);
+                if (prm.n_screens > 0) screen_crossings(prm, o, nv, t, dt, base + lane);
+#pragma unroll
+                for (int k = 0; k < 6; ++k) sto(Y0 + k, nv[k]);
+            }
+            count_add(c, SPT_CNT_LIVE_STEPS, live ? 1ull : 0ull);
+            t = t_new;
+            n_acc += 1;
+            const double tol = 1e-9 * fmax(prm.t_max, 1e-30);
+            if (!exhausted && t_new >= next_cp - tol)
+                h = (prm.t_max - t_new) * prm.initial_step_fraction;
+            else
+                h = h_next;
+            if (!(t_new < prm.t_max * (1 - 1e-14))) status = SPT_GROUP_DONE;
+            if (lane == 0) {
+                atomicAdd(c.cnt + SPT_CNT_ACCEPTED, 1ull);
+                atomicAdd(c.cnt + SPT_CNT_PARTICLE_STEPS, (unsigned long long)E);
+            }
+        } else {
+            h = h_next;
+            n_rej += 1;
+        }
+        if (isnan(err)) status = SPT_GROUP_NONFINITE;
+        ++att;
+    }
+    __syncthreads();
+    flush_counters(c, prm.counters);
+}
+
+// ---------------------------------------------------------------------------
 // host-side launchers of the kernels above, instantiated per geometry kind in
 // spt_trace_<kind>.cu (kept out of the C ABI's translation unit so that the
 // kinds compile in parallel)
@@ -2267,6 +2776,7 @@ struct TraceLaunch {
     double* slots;               // big-group slots (or null)
     long long max_slots;         // largest grid: the CTAs the slot buffer holds, or a caller's cap (0: no limit)
     cudaStream_t stream;
+    bool warp_team;              // one group per warp (trace_warp_kernel), slope slots at `slots`
 };
 
 // Shared memory and grid of a trace launch; returns 0 or a cudaError_t.
@@ -2287,6 +2797,33 @@ int trace_grid(int max_group_size, int threads, int n_groups, long long max_slot
     *grid = (int)(n_groups < cap ? n_groups : cap);
     *smem = L.bytes;
     return 0;
+}
+
+// Shared memory and grid of a warp-team launch (trace_warp_kernel): as many
+// CTAs as the SMs hold, no more than the groups need, capped by max_slots.
+template <int KIND, int FORM>
+int trace_warp_grid(int threads, int n_groups, long long max_slots, size_t* smem, int* grid, int* per_sm) {
+    const size_t bytes = warp_team_smem(threads / 32);
+    auto kern = trace_warp_kernel<KIND, FORM>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return (int)e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, threads, bytes);
+    if (e != cudaSuccess) return (int)e;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long long cap = (long long)sms * (*per_sm);
+    if (max_slots > 0 && cap > max_slots) cap = max_slots;
+    const long long need = (n_groups + threads / 32 - 1) / (threads / 32);
+    *grid = (int)(need < cap ? need : cap);
+    *smem = bytes;
+    return 0;
+}
+
+template <int KIND, int FORM>
+int trace_warp_launch(const TraceLaunch& t, int grid, size_t smem) {
+    trace_warp_kernel<KIND, FORM><<<grid, t.threads, smem, t.stream>>>(*t.s, *t.p, *t.g, t.bem, t.work, t.slots);
+    return (int)cudaGetLastError();
 }
 
 template <int KIND, int FORM, int FAR>
@@ -2323,6 +2860,12 @@ int trace_dispatch(const TraceLaunch& t, int form, int far, bool launch, int* gr
         return trace_launch<KIND, F, R>(t, *grid, *smem);                                               \
     }
     if constexpr (kBem) {
+        if (t.warp_team) {
+            if (form != SPT_FORM_FP64 || far != SPT_FAR_ADAPTIVE || E > 32 || img > 0) return -1;
+            int rc = trace_warp_grid<KIND, SPT_FORM_FP64>(t.threads, n, t.max_slots, smem, grid, per_sm);
+            if (rc || !launch) return rc;
+            return trace_warp_launch<KIND, SPT_FORM_FP64>(t, *grid, *smem);
+        }
         if (form == SPT_FORM_FP64 && far == SPT_FAR_REFERENCE) SPT_TRACE_CASE(SPT_FORM_FP64, SPT_FAR_REFERENCE)
         if (form == SPT_FORM_FP64 && far == SPT_FAR_ADAPTIVE) SPT_TRACE_CASE(SPT_FORM_FP64, SPT_FAR_ADAPTIVE)
         if (form == SPT_FORM_MIXED && far == SPT_FAR_REFERENCE) SPT_TRACE_CASE(SPT_FORM_MIXED, SPT_FAR_REFERENCE)
@@ -2331,6 +2874,7 @@ int trace_dispatch(const TraceLaunch& t, int form, int far, bool launch, int* gr
         if (form == SPT_FORM_SURROGATE && far == SPT_FAR_ADAPTIVE) SPT_TRACE_CASE(SPT_FORM_SURROGATE, SPT_FAR_ADAPTIVE)
     } else {
         // no BEM field: the far rule plays no part
+        if (t.warp_team) return -1;
         if (form == SPT_FORM_FP64) SPT_TRACE_CASE(SPT_FORM_FP64, SPT_FAR_REFERENCE)
         if (form == SPT_FORM_MIXED) SPT_TRACE_CASE(SPT_FORM_MIXED, SPT_FAR_REFERENCE)
     }

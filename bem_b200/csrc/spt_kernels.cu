@@ -358,6 +358,27 @@ int trace_threads(const SptState* s, const SptTraceParams* p, int far) {
     return t;
 }
 
+// The warp team (one group per warp) serves BEM geometries without the BEM
+// image-charge force, the float64 form with the adaptive far rule, and
+// groups of at most 32 particles; SptTraceParams.team may ask for it or
+// keep the CTA team.
+bool warp_team_offered(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b, int far) {
+    return is_bem(g->kind) && b && far == SPT_FAR_ADAPTIVE && p->form == SPT_FORM_FP64 && s->max_group_size <= 32 &&
+           spt::image_scratch(*g, *b, s->max_group_size, spt::kMaxThreads) == 0;
+}
+
+// CTA width of a warp-team launch: SptTraceParams.cta_threads when it is 32,
+// 64, 128 or 256, else 256 (every width keeps the same warps per SM; wider
+// CTAs take fewer CTA slots).
+int warp_team_threads(const SptTraceParams* p) {
+    const int want = p->cta_threads;
+    return (want == 32 || want == 64 || want == 128 || want == 256) ? want : 256;
+}
+
+constexpr int kNotLaunched = -2;  // run_warp_team: the CTA team takes the launch
+
+int64_t warp_team_slot_bytes(int threads) { return (int64_t)(threads / 32) * spt::kWarpSlotDoubles * 8; }
+
 int dispatch_kind(int kind, const spt::TraceLaunch& t, int form, int far, bool launch, int* grid, size_t* smem,
                   int* per_sm) {
     switch (kind) {
@@ -374,9 +395,77 @@ int dispatch_kind(int kind, const spt::TraceLaunch& t, int form, int far, bool l
 // first 256 bytes, then (groups above 256 particles) per-CTA slope buffers,
 // scratch_bytes in all; the persistent grid is capped by the buffers it holds
 // and by SptTraceParams.max_ctas.
+// Grid of a warp-team launch on this device (the whole GPU, or the groups,
+// or SptTraceParams.max_ctas); without a device, SMs x two CTAs.
+int warp_team_grid(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b, int far) {
+    spt::TraceLaunch t{};
+    t.s = s;
+    t.p = p;
+    t.g = g;
+    t.bem = *b;
+    t.threads = warp_team_threads(p);
+    t.warp_team = true;
+    t.max_slots = p->max_ctas > 0 ? p->max_ctas : 0;
+    int grid = 0, per_sm = 0;
+    size_t smem = 0;
+    if (dispatch_kind(g->kind, t, p->form, far, false, &grid, &smem, &per_sm) == 0 && grid > 0) return grid;
+    cudaGetLastError();  // no device: clear the error of the query
+    const int nw = t.threads / 32;
+    long long cap = 148LL * (65536 / (128 * t.threads));
+    if (p->max_ctas > 0 && cap > p->max_ctas) cap = p->max_ctas;
+    const long long need = (s->n_groups + nw - 1) / nw;
+    return (int)(need < cap ? need : cap);
+}
+
+// One warp-team launch: slope slots after the work-queue counter, grid
+// capped by the slots the scratch holds.  Returns kNotLaunched when the
+// team was not asked for and the scratch holds fewer slots than a full grid.
+int run_warp_team(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b, int far,
+                  unsigned char* scratch, int64_t scratch_bytes, cudaStream_t stream, const char* who) {
+    spt::TraceLaunch t{};
+    t.s = s;
+    t.p = p;
+    t.g = g;
+    t.bem = *b;
+    t.threads = warp_team_threads(p);
+    t.work = reinterpret_cast<int*>(scratch);
+    t.stream = stream;
+    t.warp_team = true;
+    t.slots = reinterpret_cast<double*>(scratch + 256);
+    const long long avail = scratch_bytes > 256 ? (scratch_bytes - 256) / warp_team_slot_bytes(t.threads) : 0;
+    const int full = warp_team_grid(s, p, g, b, far);
+    if (avail < full && p->team != SPT_TEAM_WARP) return kNotLaunched;
+    if (avail < 1)
+        return fail(SPT_ERR_ARG, "%s: scratch of %lld bytes holds no warp-team slot of %lld bytes", who,
+                    (long long)scratch_bytes, (long long)warp_team_slot_bytes(t.threads));
+    t.max_slots = avail;
+    if (p->max_ctas > 0 && t.max_slots > p->max_ctas) t.max_slots = p->max_ctas;
+    int grid = 0, per_sm = 0;
+    size_t smem = 0;
+    int rc = dispatch_kind(g->kind, t, p->form, far, false, &grid, &smem, &per_sm);
+    if (rc) return fail(SPT_ERR_CUDA, "%s: warp-team launch setup: %s", who, cudaGetErrorString((cudaError_t)rc));
+    if (per_sm < 1) return fail(SPT_ERR_CAPACITY, "%s: warp team of %d threads does not fit an SM", who, t.threads);
+    rc = cuda_check(cudaMemsetAsync(t.work, 0, sizeof(int), stream), "cudaMemsetAsync");
+    if (rc) return rc;
+    rc = dispatch_kind(g->kind, t, p->form, far, true, &grid, &smem, &per_sm);
+    if (rc) return fail(SPT_ERR_CUDA, "%s: trace_warp_kernel launch: %s", who, cudaGetErrorString((cudaError_t)rc));
+    return SPT_OK;
+}
+
 int run_trace(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b,
               unsigned char* scratch, int64_t scratch_bytes, cudaStream_t stream, const char* who) {
     const int far = far_rule_of(g, b);
+    if (p->team != SPT_TEAM_AUTO && p->team != SPT_TEAM_CTA && p->team != SPT_TEAM_WARP)
+        return fail(SPT_ERR_ARG, "%s: unknown team %d", who, p->team);
+    const bool warp_ok = warp_team_offered(s, p, g, b, far);
+    if (p->team == SPT_TEAM_WARP && !warp_ok)
+        return fail(SPT_ERR_ARG,
+                    "%s: the warp team needs a BEM geometry without the image-charge force, the float64 form, the "
+                    "adaptive far rule and groups of at most 32 particles", who);
+    if (warp_ok && p->team != SPT_TEAM_CTA) {
+        const int rc = run_warp_team(s, p, g, b, far, scratch, scratch_bytes, stream, who);
+        if (rc != kNotLaunched) return rc;
+    }
     const spt::Layout L = spt::make_layout(s->max_group_size, far, p->form == SPT_FORM_SURROGATE);
     spt::TraceLaunch t{};
     t.s = s;
@@ -434,6 +523,12 @@ int spt_trace_workspace_bytes(const SptState* s, const SptTraceParams* p, const 
     int64_t n = 256;
     // groups above 256 particles: one slope buffer per CTA, two 256-thread CTAs per SM
     if (L.big) n += (int64_t)sms * 2 * (int64_t)spt::big_slot_doubles(s->max_group_size) * 8;
+    // the warp team: one slot per warp of its whole grid
+    const int far = far_rule_of(g, b);
+    if (p->team != SPT_TEAM_CTA && warp_team_offered(s, p, g, b, far)) {
+        const int64_t w = 256 + (int64_t)warp_team_grid(s, p, g, b, far) * warp_team_slot_bytes(warp_team_threads(p));
+        if (w > n) n = w;
+    }
     *bytes = n;
     return SPT_OK;
 }

@@ -202,6 +202,7 @@ class Tracer:
         self.round_points = 0  # far-sum points per round (0: the kernel's default, 4); see autotune
         self.cta_threads = 0   # CTA width, 32/64/128/256 (0: the library's choice by group size); see autotune
         self.kappa_max = 0.0   # mixed form's conditioning bound for float32 sums (0: the kernel's default, 16)
+        self.team = _lib.TEAM_AUTO  # one group per warp where offered (TEAM_WARP), or per CTA (TEAM_CTA)
         self.bem = None
         if self.tables is not None:
             kw = {k: v for k, v in (("ratio4", ratio4), ("ratio2", ratio2), ("ratio_run", ratio_run)) if v is not None}
@@ -216,8 +217,10 @@ class Tracer:
 
     def params(self, t_max, rtol, atol, plummer_radius, charge_to_mass, max_attempts, log=None,
                safety=0.9, min_factor=0.2, max_factor=10.0, initial_step_fraction=1e-6,
-               coulomb_constant=COULOMB_CONSTANT, records=None, round_points=None, kappa_max=None, cta_threads=None):
+               coulomb_constant=COULOMB_CONSTANT, records=None, round_points=None, kappa_max=None, cta_threads=None,
+               team=None):
         p = _lib.SptTraceParams()
+        p.team = int(self.team if team is None else team)
         p.round_points = int(self.round_points if round_points is None else round_points)
         p.cta_threads = int(self.cta_threads if cta_threads is None else cta_threads)
         p.kappa_max = float(self.kappa_max if kappa_max is None else kappa_max)

@@ -363,11 +363,18 @@ def combine_ranks(t_total, particle_steps, world, device):
     return float(tt.item()), float(st.item())
 
 
+TEAMS = dict(auto=0, cta=1, warp=2)
+TEAM_NAMES = {0: "library's choice (one group per warp where offered)", 1: "one group per CTA",
+              2: "one group per warp"}
+
+
 def make_tracer(args, wl, dev, form=None, far_rule=None):
     from bem_b200 import engine
     tr = engine.Tracer(wl["geometry"], device=dev, form=form or args.form, z_max=wl["z_max"],
                        far_rule=far_rule or args.far_rule)
     tr.kappa_max = args.kappa
+    if form is None and far_rule is None:
+        tr.team = TEAMS[args.team]
     return tr
 
 
@@ -431,6 +438,8 @@ def run_gpu(args, rank, world):
         res = autotune.tune(tracer, pos, vel, tb, q, m, sizes, t_max, wl["rtol"], wl["atol"], 1e-12, cm,
                             threads=threads)
         autotune.apply(res, tracer)
+        if args.team != "auto":
+            tracer.team = TEAMS[args.team]
         args.tuned_config = res
         tuned = dict(res, seconds=round(time.perf_counter() - t0, 2),
                      timings={k: (round(v) if isinstance(v, float) else v) for k, v in res.get("timings", {}).items()})
@@ -491,6 +500,7 @@ def run_gpu(args, rank, world):
     return dict(value=steps_all / t_max_ranks, live=live_all / t_max_ranks, t_total=t_max_ranks, times=times,
                 counters=dc, clocks=clk.summary(), e2e=e2e, peak=peak, achieved=achieved, config=wl["config"],
                 plain=plain, accuracy=acc, tuned=tuned, t_max=t_max, ranges=ranges, image_force=img,
+                team=TEAM_NAMES[tracer.team],
                 launches_per_step=len(run.plan) if run.plan else 1)
 
 
@@ -725,6 +735,9 @@ def main():
     ap.add_argument("--far-rule", default="adaptive", choices=["reference", "adaptive"],
                     help="far-field quadrature of the BEM sum (adaptive: whole-segment Gauss-4/2 when distant)")
     ap.add_argument("--cta-threads", type=int, default=0, help="CTA width (0: autotuned, or the library's choice)")
+    ap.add_argument("--team", default="auto", choices=list(TEAMS),
+                    help="one group per warp (groups <= 32, float64 + adaptive rule) or per CTA; auto: autotuned "
+                         "where both are offered, else the library's choice")
     ap.add_argument("--bins", action="store_true",
                     help="size-binned scheduling: one launch per group-size bin on concurrent streams")
     ap.add_argument("--cpu-attempts", type=int, default=16)
@@ -778,6 +791,7 @@ def main():
         config=dict(r["config"], form=args.form, far_rule=args.far_rule, span=span, t_end=r["t_max"],
                     kappa_max=args.kappa or 16.0, autotuned=r["tuned"], size_binned=bool(args.bins),
                     cta_threads=(r["tuned"] or {}).get("cta_threads") or args.cta_threads or "library default",
+                    team=r["team"],
                     parallelism=f"contiguous group ranges balanced by cost, {world} GPU(s)",
                     l2="flushed between steps (256 MiB write); each step timed alone with CUDA events"),
         live_particle_steps_per_s=r["live"],

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define SPT_ABI_VERSION 3
+#define SPT_ABI_VERSION 4
 
 /* return codes */
 #define SPT_OK 0
@@ -63,6 +63,11 @@ extern "C" {
 #define SPT_GROUP_DONE 2     /* t >= t_max (1 - 1e-14)  (batched_rk45.py:317) */
 #define SPT_GROUP_NONFINITE 3/* the error norm became NaN: group stopped */
 #define SPT_GROUP_TIMEOUT 4  /* a bounded device wait gave up (TMA tile never arrived) */
+
+/* SptTraceParams.team */
+#define SPT_TEAM_AUTO 0
+#define SPT_TEAM_CTA 1
+#define SPT_TEAM_WARP 2
 
 /* device counters (SptTraceParams.counters, accumulated, uint64) */
 #define SPT_CNT_ATTEMPTS 0           /* group-step attempts */
@@ -310,7 +315,14 @@ typedef struct {
      * resident CTAs).  Launches of different group-size bins on concurrent
      * streams share the SMs by giving each a grid in proportion to its work. */
     int32_t max_ctas;
-    int32_t reserved3;
+    /* Team that advances one group: SPT_TEAM_AUTO (0) lets the library
+     * choose; SPT_TEAM_CTA (1) keeps one group per CTA; SPT_TEAM_WARP (2)
+     * asks for one group per warp (lane i = particle i, several groups per
+     * CTA, no CTA barrier inside a group's step), offered for BEM geometries
+     * without the BEM image-charge force, groups of at most 32 particles,
+     * the float64 form and the adaptive far rule -- the case AUTO gives to
+     * the warp team whenever the workspace holds its slope slots. */
+    int32_t team;
 } SptTraceParams;
 
 /* Scratch bytes spt_trace needs for this state/geometry (work-queue

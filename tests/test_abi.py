@@ -30,7 +30,7 @@ def test_library_loads_and_exports_every_symbol():
     lib = _lib.lib()
     for name in declared_functions():
         assert hasattr(lib, name), name
-    assert lib.spt_abi_version() == _lib.ABI_VERSION == 3
+    assert lib.spt_abi_version() == _lib.ABI_VERSION == 4
 
 
 STRUCTS = {

@@ -106,3 +106,22 @@ def test_other_entry_points_reject_null_arguments():
     assert L.spt_bem_field(None, None, None, 0, None, 0, None, None, None, None) == _lib.SPT_OK  # n = 0
     rc = L.spt_surrogate_field(FAKE, FAKE, FAKE, 4, ctypes.byref(_bem()), None, FAKE, FAKE, FAKE, None)
     assert rc == _lib.SPT_ERR_ARG
+
+
+def test_unknown_team():
+    p = _params()
+    p.team = 7
+    assert _trace(_state(), p, _geom()) == _lib.SPT_ERR_ARG
+    assert "unknown team" in _lib.last_error()
+
+
+@pytest.mark.parametrize("form,kind,size", [(_lib.FORM_FP64, _lib.GEOM_FLAT, 32),
+                                            (_lib.FORM_MIXED, _lib.GEOM_FLAT, 32)])
+def test_warp_team_where_not_offered(form, kind, size):
+    """One group per warp serves BEM geometries in the float64 form with the
+    adaptive far rule and groups of at most 32 particles; asked for anywhere
+    else, the call fails before any device work."""
+    p = _params(form)
+    p.team = _lib.TEAM_WARP
+    assert _trace(_state(max_size=size), p, _geom(kind)) == _lib.SPT_ERR_ARG
+    assert "warp team needs" in _lib.last_error()
