@@ -207,7 +207,10 @@ def apply(config, tracer, batch=None):
     """Set a tuned configuration on a Tracer (and a GroupBatch's order)."""
     tracer.round_points = int(config["round_points"])
     tracer.cta_threads = int(config.get("cta_threads", 0))
-    tracer.team = int(config.get("team", _lib.TEAM_AUTO))
+    # the warp team as the library's choice: it takes launches whose groups fill
+    # every resident warp (and only the forms it serves), the CTA team the rest
+    team = int(config.get("team", _lib.TEAM_AUTO))
+    tracer.team = _lib.TEAM_CTA if team == _lib.TEAM_CTA else _lib.TEAM_AUTO
     if tracer.tables is not None:
         r = config["ratios"]
         tracer.bem = tracer.tables.view(tracer.far_rule, ratio4=r[0], ratio2=r[1], ratio_run=r[2])

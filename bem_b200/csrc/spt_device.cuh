@@ -713,6 +713,10 @@ __device__ bool far_adaptive_warp(Ctx& c, int r0, int np_, unsigned long long& f
     const bool use_cl = NP == 1 && b.blk && b.clusters && b.cluster_kappa > 0.0 && n_run <= SPT_MAX_CLUSTER_RUNS;
     if (use_cl) {
         const int nt = b.cluster_terms, rec_len = nt + 2;
+        // the covering clusters' heads, listed first (the segment lists are free
+        // until the chunk loop) and then expanded in one lane-parallel pass
+        int* const heads = lists;
+        int n_heads = 0;
         for (int qb = 0; qb < n_run; qb += 32) {
             const int q = qb + lane;
             int lv = -1, idx = 0;
@@ -731,13 +735,18 @@ __device__ bool far_adaptive_warp(Ctx& c, int r0, int np_, unsigned long long& f
             }
             const unsigned cov = __ballot_sync(0xffffffffu, lv >= 0);
             if (lane == 0) covered[qb >> 5] = cov;
-            if (lv >= 0 && (q & ((1 << lv) - 1)) == 0) {
-                double er, ez;
-                cluster_field(b.clusters + (size_t)idx * rec_len, nt, pr[0], pz[0], er, ez);
-                ar[0] += er;
-                az[0] += ez;
-                ++cl_evals;
-            }
+            const bool head = lv >= 0 && (q & ((1 << lv) - 1)) == 0;
+            const unsigned hm = __ballot_sync(0xffffffffu, head);
+            if (head) heads[n_heads + __popc(hm & lt)] = idx;
+            n_heads += __popc(hm);
+        }
+        __syncwarp();
+        for (int hh = lane; hh < n_heads; hh += 32) {
+            double er, ez;
+            cluster_field(b.clusters + (size_t)heads[hh] * rec_len, nt, pr[0], pz[0], er, ez);
+            ar[0] += er;
+            az[0] += ez;
+            ++cl_evals;
         }
         __syncwarp();
     }
@@ -2814,7 +2823,7 @@ int trace_warp_grid(int threads, int n_groups, long long max_slots, size_t* smem
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     long long cap = (long long)sms * (*per_sm);
     if (max_slots > 0 && cap > max_slots) cap = max_slots;
-    const long long need = (n_groups + threads / 32 - 1) / (threads / 32);
+    const long long need = ((long long)n_groups + threads / 32 - 1) / (threads / 32);
     *grid = (int)(need < cap ? need : cap);
     *smem = bytes;
     return 0;

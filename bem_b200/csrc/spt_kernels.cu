@@ -413,13 +413,15 @@ int warp_team_grid(const SptState* s, const SptTraceParams* p, const SptGeometry
     const int nw = t.threads / 32;
     long long cap = 148LL * (65536 / (128 * t.threads));
     if (p->max_ctas > 0 && cap > p->max_ctas) cap = p->max_ctas;
-    const long long need = (s->n_groups + nw - 1) / nw;
+    const long long need = ((long long)s->n_groups + nw - 1) / nw;
     return (int)(need < cap ? need : cap);
 }
 
 // One warp-team launch: slope slots after the work-queue counter, grid
-// capped by the slots the scratch holds.  Returns kNotLaunched when the
-// team was not asked for and the scratch holds fewer slots than a full grid.
+// capped by the slots the scratch holds.  Returns kNotLaunched when the team
+// was not asked for (SPT_TEAM_AUTO) and either the groups do not fill every
+// resident warp of the launch at least once (fewer groups are spread wider by
+// one group per CTA) or the scratch holds fewer slots than a full grid.
 int run_warp_team(const SptState* s, const SptTraceParams* p, const SptGeometry* g, const SptBem* b, int far,
                   unsigned char* scratch, int64_t scratch_bytes, cudaStream_t stream, const char* who) {
     spt::TraceLaunch t{};
@@ -434,7 +436,13 @@ int run_warp_team(const SptState* s, const SptTraceParams* p, const SptGeometry*
     t.slots = reinterpret_cast<double*>(scratch + 256);
     const long long avail = scratch_bytes > 256 ? (scratch_bytes - 256) / warp_team_slot_bytes(t.threads) : 0;
     const int full = warp_team_grid(s, p, g, b, far);
-    if (avail < full && p->team != SPT_TEAM_WARP) return kNotLaunched;
+    if (p->team != SPT_TEAM_WARP) {
+        // the launch's resident CTAs, were there groups for all of them
+        SptState many = *s;
+        many.n_groups = 1 << 30;
+        const long long resident = warp_team_grid(&many, p, g, b, far);
+        if ((long long)s->n_groups < resident * (t.threads / 32) || avail < full) return kNotLaunched;
+    }
     if (avail < 1)
         return fail(SPT_ERR_ARG, "%s: scratch of %lld bytes holds no warp-team slot of %lld bytes", who,
                     (long long)scratch_bytes, (long long)warp_team_slot_bytes(t.threads));

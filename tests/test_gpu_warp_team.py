@@ -73,9 +73,11 @@ def _same_trace(a, b, t_max):
         assert np.all(np.abs(a["t_death"][dead] - b["t_death"][dead]) <= 1e-6 * np.abs(b["t_death"][dead]))
 
 
-def test_warp_team_matches_cta_team_and_is_the_automatic_choice():
+def test_warp_team_matches_cta_team():
     """64 groups of 32 and 32 groups of 1 to 31 particles on the 2000-panel
-    C1 capsule, traced to 2 ps by both teams and by the automatic choice."""
+    C1 capsule, traced to 2 ps by both teams.  So few groups leave most of
+    the GPU's warps without one, so the library's own choice is the CTA
+    team (bit for bit)."""
     g, geo = _c1()
     rng = np.random.default_rng(5)
     sizes = np.concatenate([np.full(64, 32), rng.integers(1, 32, 32)])
@@ -85,12 +87,35 @@ def test_warp_team_matches_cta_team_and_is_the_automatic_choice():
     auto = _trace(geo, _lib.TEAM_AUTO, pos, vel, tb, sizes, t_max)
     cta = _trace(geo, _lib.TEAM_CTA, pos, vel, tb, sizes, t_max)
     for k in ("pos", "vel", "t_death", "t", "att"):
-        np.testing.assert_array_equal(auto[k], warp[k], err_msg=k)
+        np.testing.assert_array_equal(auto[k], cta[k], err_msg=k)
     _same_trace(warp, cta, t_max)
     # the same BEM work: ring evaluations per accepted particle-step within 1 %
     rw = warp["counters"]["ring_far"] / warp["counters"]["particle_steps"]
     rc = cta["counters"]["ring_far"] / cta["counters"]["particle_steps"]
     assert abs(rw / rc - 1.0) < 0.01
+
+
+def test_automatic_choice_is_the_warp_team_when_the_groups_fill_the_gpu():
+    """As many groups of 32 as the GPU holds warps (SMs x 16), four attempts
+    each: the library's own choice is the warp team, bit for bit."""
+    g, geo = _c1()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    pos, vel, tb, sizes = _groups(g, np.full(16 * sms, 32), seed=14)
+    n = len(pos)
+    out = {}
+    for team in (_lib.TEAM_WARP, _lib.TEAM_AUTO, _lib.TEAM_CTA):
+        tr = engine.Tracer(geo, form="fp64", far_rule="adaptive", z_max=1e-3)
+        tr.team = team
+        b = engine.GroupBatch(pos, vel, tb, np.full(n, gu.Q_E), np.full(n, gu.M_E), sizes)
+        tr.launch(b, tr.params(2e-12, 1e-9, 1e-12, 1e-12, gu.CM, 4))
+        torch.cuda.synchronize()
+        out[team] = (b.positions().cpu().numpy(), b.velocities().cpu().numpy(), b.t.cpu().numpy(),
+                     (b.n_accepted + b.n_rejected).cpu().numpy())
+    for a, b in zip(out[_lib.TEAM_AUTO], out[_lib.TEAM_WARP]):
+        np.testing.assert_array_equal(a, b)
+    assert np.all(out[_lib.TEAM_WARP][3] == 4)
+    # the CTA team's pair sums add in another order: same steps, last digits
+    np.testing.assert_allclose(out[_lib.TEAM_CTA][2], out[_lib.TEAM_WARP][2], rtol=1e-6)
 
 
 def test_warp_team_screens_and_outputs_match_cta_team():
@@ -164,3 +189,16 @@ def test_autotuner_offers_the_team_choice():
     assert "team=warp" in res["timings"] and "team=cta" in res["timings"]
     mixed = engine.Tracer(geo, form="mixed", far_rule="adaptive", z_max=1e-3)
     assert not autotune.warp_team_offered(mixed, sizes)
+
+
+def test_tuned_warp_team_is_not_applied_to_other_forms():
+    g, geo = _c1()
+    cfg = dict(team=_lib.TEAM_WARP, cta_threads=256, round_points=4, ratios=[8.0, 300.0, 4.0], order="largest_first")
+    mixed = engine.Tracer(geo, form="mixed", far_rule="adaptive", z_max=1e-3)
+    autotune.apply(cfg, mixed)
+    assert mixed.team == _lib.TEAM_AUTO
+    fp64 = engine.Tracer(geo, form="fp64", far_rule="adaptive", z_max=1e-3)
+    autotune.apply(cfg, fp64)
+    assert fp64.team == _lib.TEAM_AUTO  # the library then gives the warp team the launches it fills
+    autotune.apply(dict(cfg, team=_lib.TEAM_CTA), fp64)
+    assert fp64.team == _lib.TEAM_CTA
