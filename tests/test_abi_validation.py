@@ -125,3 +125,31 @@ def test_warp_team_where_not_offered(form, kind, size):
     p.team = _lib.TEAM_WARP
     assert _trace(_state(max_size=size), p, _geom(kind)) == _lib.SPT_ERR_ARG
     assert "warp team needs" in _lib.last_error()
+
+
+def _workspace(state, params, geom, bem):
+    n = ctypes.c_int64(0)
+    rc = _lib.lib().spt_trace_workspace_bytes(ctypes.byref(state), ctypes.byref(params), ctypes.byref(geom),
+                                              ctypes.byref(bem), ctypes.byref(n))
+    assert rc == _lib.SPT_OK
+    return n.value
+
+
+def test_workspace_holds_the_warp_teams_slots():
+    """Groups of at most 32 in the float64 form with the adaptive rule: the
+    workspace holds one step slot (54 doubles a particle, 32 lanes) per warp
+    of the warp team's grid -- without a device, SMs x two 256-thread CTAs,
+    no more than the groups need; one group per CTA needs only the queue
+    counter."""
+    geom = _geom(_lib.GEOM_POST_BEM)
+    bem = _bem(far_rule=_lib.FAR_ADAPTIVE)
+    slot = 54 * 32 * 8
+    p = _params()
+    n = _workspace(_state(n_groups=4096, max_size=32), p, geom, bem)
+    assert n == 256 + 148 * 2 * 8 * slot
+    assert _workspace(_state(n_groups=20, max_size=32), p, geom, bem) == 256 + 3 * 8 * slot
+    p.team = _lib.TEAM_CTA
+    assert _workspace(_state(n_groups=4096, max_size=32), p, geom, bem) == 256
+    p.team = _lib.TEAM_AUTO
+    assert _workspace(_state(n_groups=4096, max_size=33), p, geom, bem) == 256
+    assert _workspace(_state(n_groups=4096, max_size=32), _params(_lib.FORM_MIXED), geom, bem) == 256
