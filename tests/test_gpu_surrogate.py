@@ -196,8 +196,9 @@ def test_learned_form_measured_against_chosen_form():
     2M training points log-uniform 1 nm - 1 mm from the surface, labelled by
     the float64 BEM evaluator; Adam, lr 1e-3 cosine, 20k steps, batch 8192;
     exact BEM within 5 nm, 1 % spot checks) on the C1 tip, against the chosen
-    form (float32 + Kahan, adaptive far rule, no network), both tracing 148
-    C4-sized groups (sizes logU[1, 128], seed 4) to t = 0.1 ps.  Measured:
+    form (float64, adaptive far rule, no network) and the float32 form
+    (float32 + Kahan, adaptive far rule), all tracing 148 C4-sized groups
+    (sizes logU[1, 128], seed 4) to t = 0.1 ps.  Measured:
     CUDA-event time to reach t_end, attempts, accepted particle-steps and the
     endpoint error against the plain float64 form.  Particle-steps per second
     alone would reward a form that takes more, smaller steps, so the verdict
@@ -220,7 +221,8 @@ def test_learned_form_measured_against_chosen_form():
     n = len(pos)
     t_end = 0.1e-12
     out = {}
-    for name, form, rule, kw in (("plain", "fp64", "reference", {}), ("chosen", "mixed", "adaptive", {}),
+    for name, form, rule, kw in (("plain", "fp64", "reference", {}), ("chosen", "fp64", "adaptive", {}),
+                                 ("mixed", "mixed", "adaptive", {}),
                                  ("learned", "surrogate", "adaptive", dict(surrogate=model, band=5e-9, spot=0.01))):
         tr = engine.Tracer(geo, form=form, far_rule=rule, z_max=1e-3, **kw)
         b = engine.GroupBatch(pos, vel, d["t"], np.full(n, gu.Q_E), np.full(n, gu.M_E), d["group_sizes"])
@@ -233,7 +235,7 @@ def test_learned_form_measured_against_chosen_form():
                          td=b.t_death.cpu().numpy())
     ref = out["plain"]
     alive = np.isinf(ref["td"])
-    for name in ("chosen", "learned"):
+    for name in ("chosen", "mixed", "learned"):
         o = out[name]
         ok = alive & np.isinf(o["td"])
         o["err"] = float((np.linalg.norm(o["pos"] - ref["pos"], axis=-1)[ok] /
