@@ -482,9 +482,9 @@ def gen_trace_c1():
 def gen_trace_c2():
     """C2 scale: one group of 1024 from the C2 sampler (seed 2) on the C1
     tip, every member born at t = 0 (so all 1024 interact from the first
-    stage), traced to t = 0.2 fs (with 1024 electrons 1 nm apart the step
-    stays near 1e-17 s, so a longer trace takes the reference hours: its
-    field of 1024 points takes ~10 s a stage).  Traced to t_max, not cut
+    stage), traced to t = 2e-18 s (with 1024 electrons 1 nm apart the
+    reference's steps stay near 5e-19 s, and its field of 1024 points takes
+    ~12 s a stage, so a longer trace takes it hours).  Traced to t_max, not cut
     after a number of attempts: both runs end at the same time, so the
     endpoints do not carry the step sizes' last digits (a budget-cut run's
     end time does).  The sites are lifted 1 nm off the apex
@@ -500,7 +500,7 @@ def gen_trace_c2():
     apex = np.array([0.0, 0.0, geo.L])
     nrm = (pos - apex) / np.linalg.norm(pos - apex, axis=-1, keepdims=True)
     pos = pos + 1e-9 * nrm
-    res = _trace_groups(geo, pos, vel, tb, 0.2e-15, 1e-9, 1e-12, 1e-3)
+    res = _trace_groups(geo, pos, vel, tb, 2e-18, 1e-9, 1e-12, 1e-3)
     _save("trace_c2", **_post_fields(geo, g), **res)
 
 

@@ -6,7 +6,7 @@ trace_c3_s*, trace_c4_s*):
   traced from emission to t = 20 ps;
 * C2: one group of 1024 on the C1 tip, every member alive from the first
   stage (the global-memory slope path of groups above 256 particles),
-  traced to t = 0.2 fs;
+  traced to t = 2e-18 s (the reference's steps are ~5e-19 s);
 * C3 / C4: uneven group sizes (1, 2, 129, 256 on the ~3000-panel well; 1,
   2, 7, 128 on the C1 tip) in ONE launch, or size-binned (one launch per
   bin on concurrent streams), each size bin compared with its own reference
