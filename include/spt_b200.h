@@ -453,6 +453,11 @@ int spt_image_force(const double* x, const double* y, const double* z, const dou
  *     groups above 256 particles the scratch holds floor((4 MiB - 256) /
  *     (432 * max_group_size)) per-CTA buffers, which caps the number of
  *     CTAs that run at once (9 at 1024 particles).
+ *   - The warp team (SptTraceParams.team) keeps 13,824 bytes per warp of
+ *     step state in the same scratch, which holds 37 CTAs of 256 threads:
+ *     SPT_TEAM_AUTO keeps one group per CTA here (the warp team takes only
+ *     launches that fill the GPU, whose grid does not fit), and an explicit
+ *     SPT_TEAM_WARP runs on those 37 CTAs.
  *   - The first call in each CUDA context (the current device's primary
  *     context, or the caller's own driver-API context) looks the array's
  *     address up (cudaGetSymbolAddress) with that device current and caches
